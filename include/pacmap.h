@@ -1,0 +1,208 @@
+/*
+ * pacmap.h -- C ABI of the B200-native PaCMAP engine (libpacmap_b200.so).
+ *
+ * Drop-in boundary for beamform/pacmap-rs v0.2.6 (crate `pacmap`). The reference's public API is Rust:
+ *   fit_transform(x: ArrayView2<f32>, config: Configuration)
+ *       -> Result<(Array2<f32>, Option<Array3<f32>>), PaCMapError>                     src/lib.rs:294-297
+ *   knn::find_k_nearest_neighbors(data: ArrayView2<f32>, k: usize)
+ *       -> (Array2<u32>, Array2<f32>)                                                   src/knn.rs:137
+ * Each entry point below names the reference item it replaces. A Rust (or any FFI) binding wraps these
+ * with the reference's types; the Python mirror in pacmap-rs_b200/pacmap_b200 does exactly that.
+ *
+ * Conventions (as in the reference, src/lib.rs:294-367): synchronous; inputs borrowed; every matrix is
+ * row-major and dense; outputs go to caller-owned buffers of the documented size; errors are status
+ * codes (the reference's Result), with a thread-local message from pacmap_last_error(). All compute runs
+ * on one CUDA device (cfg->device); there is no CPU fallback: without a usable sm_100 device every
+ * compute entry point returns PACMAP_ERR_NO_DEVICE. Calls from several host threads are safe; calls on
+ * one device are serialised.
+ */
+#ifndef PACMAP_B200_H
+#define PACMAP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* PaCMapError (src/lib.rs:870-922) and KnnError (src/knn.rs:196-206), one code per variant, plus the
+ * conditions the reference turns into panics or endless loops, and device-side failures. */
+typedef enum pacmap_status {
+  PACMAP_OK = 0,
+  PACMAP_ERR_SAMPLE_SIZE = 1,               /* SampleSize: n <= 1                       lib.rs:875 */
+  PACMAP_ERR_INVALID_NN_SHAPE = 2,          /* InvalidNearestNeighborShape              lib.rs:879 */
+  PACMAP_ERR_EMPTY_ARRAY_MEAN = 3,          /* EmptyArrayMean                           lib.rs:888 */
+  PACMAP_ERR_NORMAL = 4,                    /* Normal (distribution construction)       lib.rs:892 */
+  PACMAP_ERR_INVALID_NEIGHBOR_COUNT = 5,    /* InvalidNeighborCount                     lib.rs:896 */
+  PACMAP_ERR_INVALID_FAR_POINT_COUNT = 6,   /* InvalidFarPointCount                     lib.rs:900 */
+  PACMAP_ERR_EMPTY_ARRAY_MIN_MAX = 7,       /* EmptyArrayMinMax                         lib.rs:904 */
+  PACMAP_ERR_ZERO_RANGE = 8,                /* ZeroRange (never raised, as in the ref.) lib.rs:908 */
+  PACMAP_ERR_PCA = 9,                       /* Pca                                      lib.rs:912 */
+  PACMAP_ERR_KNN_CONSTRUCTION = 10,         /* KnnError::Construction                   knn.rs:200 */
+  PACMAP_ERR_KNN_RESERVATION = 11,          /* KnnError::Reservation                    knn.rs:204 */
+  PACMAP_ERR_MISSING_TRANSFORM = 12,        /* MissingTransform                         lib.rs:920 */
+  PACMAP_ERR_INVALID_ARGUMENT = 20,         /* NULL pointer / bad enum / size overflow               */
+  PACMAP_ERR_PAIR_INDEX = 21,               /* a provided pair names a point >= n (the ref. panics)  */
+  PACMAP_ERR_SAMPLING = 22,                 /* distinct partners cannot be drawn (the ref. spins)    */
+  PACMAP_ERR_UNSUPPORTED = 23,              /* Initialization::Pca, or a size beyond a kernel limit  */
+  PACMAP_ERR_CUDA = 30,                     /* CUDA runtime error (message has the detail)           */
+  PACMAP_ERR_OOM = 31,                      /* device allocation failed                              */
+  PACMAP_ERR_NO_DEVICE = 32,                /* no CUDA device of compute capability 10.x             */
+  PACMAP_ERR_DEVICE_INVARIANT = 33          /* a kernel's own check failed (index range, timeout)    */
+} pacmap_status;
+
+/* Initialization (src/lib.rs:226-239). PCA is not built: PACMAP_ERR_UNSUPPORTED. */
+typedef enum pacmap_init_kind {
+  PACMAP_INIT_PCA = 0,
+  PACMAP_INIT_VALUE = 1,  /* Value(Array2<f32>): init_value, n x embedding_dimensions           */
+  PACMAP_INIT_RANDOM = 2  /* Random(Option<u64>): init_has_seed / init_seed                     */
+} pacmap_init_kind;
+
+/* PairConfiguration (src/lib.rs:241-267). */
+typedef enum pacmap_pair_kind {
+  PACMAP_PAIRS_GENERATE = 0,
+  PACMAP_PAIRS_NEIGHBORS_PROVIDED = 1,  /* pair_neighbors: (n*k) x 2                               */
+  PACMAP_PAIRS_ALL_PROVIDED = 2         /* pair_neighbors, pair_mn, pair_fp: rows x 2 each          */
+} pacmap_pair_kind;
+
+/* How the exact kNN is computed (no reference analogue; every mode returns the same indices). */
+typedef enum pacmap_knn_mode {
+  PACMAP_KNN_AUTO = 0,         /* tensor-core filter when the dimension allows it, else SIMT exact   */
+  PACMAP_KNN_TENSOR_F16 = 1,   /* tcgen05 FP16 distance GEMM filter + exact FP32 re-rank            */
+  PACMAP_KNN_TENSOR_BF16 = 2,  /* tcgen05 BF16 distance GEMM filter + exact FP32 re-rank            */
+  PACMAP_KNN_SIMT_EXACT = 3    /* every distance in the reference's FP32 order on CUDA cores        */
+} pacmap_knn_mode;
+
+/* Configuration (src/lib.rs:159-224), field by field, plus the engine's switches at the end.
+ * Option<T> fields are a has_ flag plus the value. Pointers are host memory and only read. */
+typedef struct pacmap_config {
+  uint64_t embedding_dimensions;       /* default 2                                                  */
+  int32_t init_kind;                   /* pacmap_init_kind, default PCA (as the reference)          */
+  const float* init_value;             /* VALUE: n x embedding_dimensions                           */
+  int32_t init_has_seed;               /* RANDOM(Some(seed)) when 1, RANDOM(None) when 0            */
+  uint64_t init_seed;
+  float mid_near_ratio;                /* default 0.5                                                */
+  float far_pair_ratio;                /* default 2.0                                                */
+  int32_t has_override_neighbors;      /* override_neighbors: Option<usize>                          */
+  uint64_t override_neighbors;
+  int32_t has_seed;                    /* seed: Option<u64> (pair sampling)                          */
+  uint64_t seed;
+  int32_t pair_kind;                   /* pacmap_pair_kind, default GENERATE                        */
+  const uint32_t* pair_neighbors;      /* NEIGHBORS_PROVIDED / ALL_PROVIDED                         */
+  uint64_t pair_neighbors_rows;
+  const uint32_t* pair_mn;             /* ALL_PROVIDED                                               */
+  uint64_t pair_mn_rows;
+  const uint32_t* pair_fp;             /* ALL_PROVIDED                                               */
+  uint64_t pair_fp_rows;
+  float learning_rate;                 /* default 1.0                                                */
+  uint64_t num_iters[3];               /* default (100, 100, 250)                                    */
+  const uint64_t* snapshots;           /* Option<Vec<usize>>: NULL = None                            */
+  uint64_t n_snapshots;
+  uint64_t approx_threshold;           /* default 8000; accepted, the engine's kNN is always exact   */
+  /* --- engine switches (no reference analogue) --- */
+  int32_t knn_mode;                    /* pacmap_knn_mode, default AUTO                              */
+  int32_t device;                      /* CUDA device ordinal, default 0                             */
+  float* loss_trace;                   /* optional out: the loss (grad[n,0]) of every iteration      */
+} pacmap_config;
+
+/* Configuration::default() (src/lib.rs:208-224) plus the engine defaults. */
+pacmap_config pacmap_config_default(void);
+
+/* fit_transform (src/lib.rs:294-367). x: n x d. out_embedding: n x embedding_dimensions.
+ * out_snapshots: n_snapshots x n x embedding_dimensions, or NULL (ignored when cfg->snapshots is NULL).
+ * Slot semantics follow src/lib.rs:789-791,830-836: slot 0 starts as the initial embedding; iteration
+ * itr (0-based) writes the first slot whose index equals itr + 1. */
+pacmap_status pacmap_fit_transform(const float* x, uint64_t n, uint64_t d, const pacmap_config* cfg,
+                                   float* out_embedding, float* out_snapshots);
+
+/* Same as pacmap_fit_transform with x, out_embedding (and out_snapshots) in device memory of
+ * cfg->device (no reference analogue: it keeps host<->device copies out of a caller's timing). */
+pacmap_status pacmap_fit_transform_device(const float* d_x, uint64_t n, uint64_t d, const pacmap_config* cfg,
+                                          float* d_out_embedding, float* d_out_snapshots);
+
+/* knn::find_k_nearest_neighbors (src/knn.rs:137-194): exact Euclidean kNN of the rows of x (not
+ * preprocessed), self excluded, k' = min(k, n-1) columns in ascending (f32 distance, index) order.
+ * out_idx, out_dist: n x k'. n == 0 is a no-op. Distances are the reference's f32 values. */
+pacmap_status pacmap_knn_exact(const float* x, uint64_t n, uint64_t d, uint64_t k, int32_t knn_mode,
+                               int32_t device, uint32_t* out_idx, float* out_dist);
+
+/* --- stage entry points: the parity harness and callers that run part of the pipeline --- */
+
+/* preprocess_x non-PCA branch (src/lib.rs:485-511): out = (x - min) / max - column mean. x, out: n x d.
+ * out_mean: d values (may be NULL). */
+pacmap_status pacmap_preprocess(const float* x, uint64_t n, uint64_t d, int32_t device, float* out,
+                                float* out_min, float* out_max, float* out_mean);
+
+/* sample_pairs with PairConfiguration::Generate (src/lib.rs:641-648 -> src/neighbors.rs:56-108) on the
+ * raw x: preprocessing, exact kNN with k+50 candidates, sigma scaling, reselection, MN and FP sampling.
+ * Pair counts come from decide_num_pairs (src/lib.rs:565-597); out_counts receives (k, n_mn, n_fp)
+ * where k = min(n_neighbors, n-1). Buffers: out_pnn (n*k x 2), out_pmn (n*n_mn x 2), out_pfp
+ * (n*n_fp x 2); any may be NULL to only query the counts. */
+pacmap_status pacmap_generate_pairs(const float* x, uint64_t n, uint64_t d, const pacmap_config* cfg,
+                                    uint64_t* out_counts, uint32_t* out_pnn, uint32_t* out_pmn,
+                                    uint32_t* out_pfp);
+
+/* generate_pairs steps after the kNN (src/neighbors.rs:79-89, src/sampling.rs:251-286): sigma from the
+ * 4th-6th neighbour distances, scaled distances, the k best per row. knn_idx/knn_dist: n x kp.
+ * out_pnn: (n*k) x 2. out_sigma (n, may be NULL). */
+pacmap_status pacmap_reselect_neighbors(const uint32_t* knn_idx, const float* knn_dist, uint64_t n,
+                                        uint64_t kp, uint64_t k, int32_t device, uint32_t* out_pnn,
+                                        float* out_sigma);
+
+/* sample_mn_pair_deterministic / sample_fp_pair_deterministic (src/sampling.rs:77-142) on the
+ * library's Philox stream. xp: the preprocessed n x d data. out_pmn: (n*n_mn) x 2; out_pfp:
+ * (n*n_fp) x 2 given pair_neighbors ((n*k) x 2). Either output may be NULL to skip it. */
+pacmap_status pacmap_sample_pairs(const float* xp, uint64_t n, uint64_t d, const uint32_t* pair_neighbors,
+                                  uint64_t k, uint64_t n_mn, uint64_t n_fp, uint64_t seed, int32_t device,
+                                  uint32_t* out_pmn, uint32_t* out_pfp);
+
+/* The optimiser loop (src/lib.rs:800-837) from an explicit state: iterations [itr_begin, itr_end) of
+ * weights -> gradient -> Adam, starting from y, m, v (n x dim each, updated in place). The schedule
+ * (num_iters p1, p2) and lr set the weights and the bias-corrected step. out_grad (optional,
+ * (n+1) x dim): the gradient of the last iteration, loss at [n, 0]. */
+pacmap_status pacmap_optimize_steps(float* y, float* m, float* v, uint64_t n, uint64_t dim,
+                                    const uint32_t* pnn, uint64_t n_nn, const uint32_t* pmn, uint64_t n_mn,
+                                    const uint32_t* pfp, uint64_t n_fp, float learning_rate, uint64_t p1,
+                                    uint64_t p2, uint64_t itr_begin, uint64_t itr_end, int32_t device,
+                                    float* out_grad);
+
+/* pacmap_grad (src/gradient.rs:35-74) with explicit weights: out_grad ((n+1) x dim) receives the
+ * gradient of every point and the loss at [n, 0]. */
+pacmap_status pacmap_gradient(const float* y, uint64_t n, uint64_t dim, const uint32_t* pnn, uint64_t n_nn,
+                              const uint32_t* pmn, uint64_t n_mn, const uint32_t* pfp, uint64_t n_fp, float w_nn,
+                              float w_mn, float w_fp, int32_t device, float* out_grad);
+
+/* Initialization::Value (src/lib.rs:753-766) applied on the device: (v - mean) * 1e-4 / std. */
+pacmap_status pacmap_init_value(const float* v, uint64_t n, uint64_t dim, int32_t device, float* out);
+
+/* Initialization::Random(seed) on the library's Philox stream (N(0,1), Box-Muller). */
+pacmap_status pacmap_init_random(uint64_t n, uint64_t dim, uint64_t seed, int32_t device, float* out);
+
+/* Quality of an embedding (no reference analogue): mean 10-NN preservation over `sample` (n_sample
+ * point indices; neighbours by the reference's f32 distance on the preprocessed data) and random-triplet
+ * order accuracy over `triplets` (n_triplets x 3). x: raw n x d data; y: n x dim embedding. */
+pacmap_status pacmap_quality(const float* x, uint64_t n, uint64_t d, const float* y, uint64_t dim,
+                             const uint32_t* sample, uint64_t n_sample, uint64_t k, const uint32_t* triplets,
+                             uint64_t n_triplets, int32_t device, double* out_preservation,
+                             double* out_triplet_accuracy);
+
+/* Stage timing (diagnostics): when enabled, each fit_transform records the device time of its stages
+ * with CUDA events on its stream. pacmap_stage_times fills up to `cap` values in milliseconds, in the
+ * order preprocess, knn, reselect, sample_mn, sample_fp, csr, init, optimize, and returns how many. */
+void pacmap_set_stage_timing(int32_t enabled);
+uint64_t pacmap_stage_times(double* out_ms, uint64_t cap);
+
+/* Kernel launches issued by this thread since the last call of this function (diagnostics). */
+uint64_t pacmap_take_launch_count(void);
+
+/* The message of the last failure on this thread ("" after success). */
+const char* pacmap_last_error(void);
+
+/* Library version string. */
+const char* pacmap_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PACMAP_B200_H */

@@ -672,9 +672,10 @@ int orc_generate_pairs(const float* x, uint64_t n, uint64_t d, uint64_t n_neighb
 // Quality metrics (no reference analogue; the library computes the same numbers on the GPU).
 // ------------------------------------------------------------------------------------------------
 
-// Mean fraction of each sampled point's `kk` nearest neighbours in the high-dimensional data (f32
-// reference distance, ties -> lower index) that are also among its `kk` nearest neighbours in the
-// embedding (f32 squared distance summed over dims in order, ties -> lower index).
+// Mean fraction of each sampled point's `kk` nearest neighbours in the high-dimensional data that are
+// also among its `kk` nearest neighbours in the embedding. Both neighbour sets use the reference's f32
+// distance (distance.rs:50-75; in the embedding, dim < 8, that is the serial sum) ordered by
+// (sqrt distance, index), as knn.rs ranks neighbours.
 double orc_knn_preservation(const float* xh, uint64_t n, uint64_t d, const float* yl, uint64_t dim,
                             const uint32_t* sample, uint64_t n_sample, uint64_t kk) {
   double total = 0.0;
@@ -690,14 +691,14 @@ double orc_knn_preservation(const float* xh, uint64_t n, uint64_t d, const float
       bl.clear();
       for (uint64_t j = 0; j < n; ++j) {
         if (j == i) continue;
-        bh.emplace_back((static_cast<uint64_t>(total_key(ref_dist_sq(xh + i * d, xh + j * d, d))) << 32) | j,
+        bh.emplace_back((static_cast<uint64_t>(total_key(ref_dist(xh + i * d, xh + j * d, d))) << 32) | j,
                         static_cast<uint32_t>(j));
         float s = 0.0f;
         for (uint64_t c = 0; c < dim; ++c) {
           const float df = yl[i * dim + c] - yl[j * dim + c];
           s = s + df * df;
         }
-        bl.emplace_back((static_cast<uint64_t>(total_key(s)) << 32) | j, static_cast<uint32_t>(j));
+        bl.emplace_back((static_cast<uint64_t>(total_key(std::sqrt(s))) << 32) | j, static_cast<uint32_t>(j));
       }
       const uint64_t kq = std::min<uint64_t>(kk, bh.size());
       std::nth_element(bh.begin(), bh.begin() + (kq - 1), bh.end());

@@ -1,0 +1,169 @@
+// Exact kNN -- knn::find_k_nearest_neighbors (src/knn.rs:137-194).
+//
+// The reference forms all n(n-1)/2 upper-triangle f32 distances (knn.rs:149-163), sorts them globally
+// (knn.rs:166-167) and fills each row first come, first served (knn.rs:176-191). Row i therefore holds
+// its k' = min(k, n-1) smallest distances to j != i in ascending order; ties, which the reference's
+// unstable sort leaves open, go to the lower index here. This file computes the same rows without the
+// O(n^2) triple list:
+//
+//   * knn_simt_kernel: every distance in the reference's exact f32 order (distance.rs:50-75) on CUDA
+//     cores, each block keeping the running k' best (distance key, index) of 32 query rows in shared
+//     memory. Used for small n, for any d, and as the fallback for rows the tensor-core filter
+//     (knn_tc.cu) cannot settle.
+#include "engine.cuh"
+#include "knn_tc.cuh"
+
+namespace pacmap {
+namespace {
+
+constexpr int SQ_QB = 32;   // query rows per block
+constexpr int SQ_KT = 64;   // keys per tile
+constexpr int SQ_DC = 64;   // dimensions staged per pass (multiple of 8)
+constexpr int SQ_LD = SQ_DC + 4;  // smem row stride (floats): 16-byte aligned, conflict-free float4 rows
+constexpr int SQ_THREADS = 256;
+constexpr int SQ_MAX_K = 448;     // P = next_pow2(K + KT) <= 512
+
+__global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __restrict__ x, uint64_t n, int d, int K,
+                                                              int P, const uint32_t* __restrict__ rows,
+                                                              uint64_t n_rows, uint32_t* __restrict__ out_idx,
+                                                              float* __restrict__ out_dist) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* qs = reinterpret_cast<float*>(smem);
+  float* ks = qs + SQ_QB * SQ_LD;
+  uint64_t* lists = reinterpret_cast<uint64_t*>(ks + SQ_KT * SQ_LD);
+  __shared__ int stage_cnt[SQ_QB];
+  __shared__ uint64_t theta[SQ_QB];
+  __shared__ uint64_t qrow[SQ_QB];
+
+  const int tid = threadIdx.x;
+  const int kt = tid & (SQ_KT - 1);
+  const int qg = tid >> 6;  // 4 groups x 8 queries
+  const uint64_t slot0 = static_cast<uint64_t>(blockIdx.x) * SQ_QB;
+
+  if (tid < SQ_QB) {
+    stage_cnt[tid] = 0;
+    theta[tid] = ~0ull;
+    const uint64_t s = slot0 + tid;
+    qrow[tid] = (s < n_rows) ? (rows ? static_cast<uint64_t>(rows[s]) : s) : ~0ull;
+  }
+  for (int e = tid; e < SQ_QB * P; e += SQ_THREADS) lists[e] = ~0ull;
+  __syncthreads();
+
+  const int nc8 = (d / 8) * 8;  // the lane-accumulated part; the tail d % 8 is added after the lane sum
+  for (uint64_t key0 = 0; key0 < n; key0 += SQ_KT) {
+    float acc[8][8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+#pragma unroll
+      for (int l = 0; l < 8; ++l) acc[q][l] = 0.0f;
+
+    for (int dbase = 0; dbase < nc8; dbase += SQ_DC) {
+      const int dlen = min(SQ_DC, nc8 - dbase);
+      __syncthreads();
+      for (int e = tid; e < SQ_QB * dlen; e += SQ_THREADS) {
+        const int qi = e / dlen, cc = e - qi * dlen;
+        const uint64_t r = qrow[qi];
+        qs[qi * SQ_LD + cc] = (r != ~0ull) ? x[r * d + dbase + cc] : 0.0f;
+      }
+      for (int e = tid; e < SQ_KT * dlen; e += SQ_THREADS) {
+        const int kk = e / dlen, cc = e - kk * dlen;
+        const uint64_t j = key0 + kk;
+        ks[kk * SQ_LD + cc] = (j < n) ? x[j * d + dbase + cc] : 0.0f;
+      }
+      __syncthreads();
+      for (int c8 = 0; c8 < dlen; c8 += 8) {
+        const float4 k0 = *reinterpret_cast<const float4*>(&ks[kt * SQ_LD + c8]);
+        const float4 k1 = *reinterpret_cast<const float4*>(&ks[kt * SQ_LD + c8 + 4]);
+        const float kv[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float* qp = &qs[(qg * 8 + q) * SQ_LD + c8];
+          const float4 q0 = *reinterpret_cast<const float4*>(qp);
+          const float4 q1 = *reinterpret_cast<const float4*>(qp + 4);
+          const float qv[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+          for (int l = 0; l < 8; ++l) {
+            const float df = __fsub_rn(qv[l], kv[l]);
+            acc[q][l] = __fadd_rn(acc[q][l], __fmul_rn(df, df));
+          }
+        }
+      }
+    }
+
+    const uint64_t j = key0 + kt;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int qi = qg * 8 + q;
+      const uint64_t r = qrow[qi];
+      float t = 0.0f;
+#pragma unroll
+      for (int l = 0; l < 8; ++l) t = __fadd_rn(t, acc[q][l]);
+      if (r == ~0ull || j >= n || j == r) continue;
+      for (int e = nc8; e < d; ++e) {
+        const float df = __fsub_rn(x[r * d + e], x[j * d + e]);
+        t = __fadd_rn(t, __fmul_rn(df, df));
+      }
+      const float dist = __fsqrt_rn(t);
+      const uint64_t key = (static_cast<uint64_t>(total_key(dist)) << 32) | j;
+      if (key < theta[qi]) {
+        const int pos = atomicAdd(&stage_cnt[qi], 1);
+        lists[qi * P + K + pos] = key;
+      }
+    }
+    __syncthreads();
+    // Merge the staged candidates of each query into its sorted list (one warp per query).
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int qi = warp; qi < SQ_QB; qi += SQ_THREADS / 32) {
+      const int cnt = stage_cnt[qi];
+      if (cnt == 0) continue;
+      uint64_t* L = lists + qi * P;
+      for (int e = K + cnt + lane; e < P; e += 32) L[e] = ~0ull;
+      warp_bitonic_sort_u64(L, P);
+      if (lane == 0) {
+        stage_cnt[qi] = 0;
+        theta[qi] = L[K - 1];
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+
+  for (int e = tid; e < SQ_QB * K; e += SQ_THREADS) {
+    const int qi = e / K, cc = e - qi * K;
+    const uint64_t s = slot0 + qi;
+    if (s >= n_rows) continue;
+    const uint64_t key = lists[qi * P + cc];
+    out_idx[s * K + cc] = static_cast<uint32_t>(key & 0xFFFFFFFFu);
+    out_dist[s * K + cc] = key_to_float(static_cast<uint32_t>(key >> 32));
+  }
+}
+
+}  // namespace
+
+void knn_rows_simt(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, const uint32_t* d_rows,
+                   uint64_t n_rows, uint32_t* d_idx, float* d_dist) {
+  if (n_rows == 0 || kp == 0) return;
+  PM_REQUIRE(kp <= SQ_MAX_K, PACMAP_ERR_UNSUPPORTED,
+             "exact kNN supports at most " + std::to_string(SQ_MAX_K) + " neighbours per row");
+  PM_REQUIRE(n < (1ull << 32) && d < (1ull << 31), PACMAP_ERR_UNSUPPORTED, "kNN needs n < 2^32 and d < 2^31");
+  const int K = static_cast<int>(kp);
+  const int P = next_pow2(K + SQ_KT);
+  const size_t smem = static_cast<size_t>(SQ_QB + SQ_KT) * SQ_LD * sizeof(float) + static_cast<size_t>(SQ_QB) * P * 8;
+  PM_CUDA(cudaFuncSetAttribute(knn_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  knn_simt_kernel<<<ceil_div(n_rows, SQ_QB), SQ_THREADS, smem, c.stream>>>(d_x, n, static_cast<int>(d), K, P, d_rows,
+                                                                         n_rows, d_idx, d_dist);
+  PM_LAUNCHED();
+}
+
+void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, int mode, uint32_t* d_idx,
+                      float* d_dist) {
+  if (n == 0 || kp == 0) return;
+  if (mode != PACMAP_KNN_SIMT_EXACT && knn_tc_supported(n, d, kp)) {
+    if (knn_tc_device(c, d_x, n, d, kp, mode == PACMAP_KNN_TENSOR_BF16, d_idx, d_dist)) return;
+  }
+  PM_REQUIRE(mode == PACMAP_KNN_AUTO || mode == PACMAP_KNN_SIMT_EXACT, PACMAP_ERR_UNSUPPORTED,
+             "the tensor-core kNN does not support this shape (d <= 128 and k' <= 192 are required)");
+  knn_rows_simt(c, d_x, n, d, kp, nullptr, n, d_idx, d_dist);
+}
+
+}  // namespace pacmap

@@ -1,0 +1,11 @@
+// Tensor-core (tcgen05) distance-GEMM filter for the exact kNN.
+#pragma once
+#include "engine.cuh"
+
+namespace pacmap {
+// True when the tcgen05 filter handles this shape.
+bool knn_tc_supported(uint64_t n, uint64_t d, uint64_t kp);
+// Exact kNN through the tensor-core filter + FP32 re-rank; false when it declined the problem.
+bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, bool bf16, uint32_t* d_idx,
+                   float* d_dist);
+}  // namespace pacmap

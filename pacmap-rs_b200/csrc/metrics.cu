@@ -1,0 +1,68 @@
+// K14 -- embedding quality (no reference analogue; the judge of the learned initialiser):
+//   * k-NN preservation: for each sampled point, the share of its k nearest neighbours in the data
+//     (preprocessed, reference f32 distance) that are also among its k nearest in the embedding, both
+//     ranked by (f32 distance, index) with the exact kNN kernel;
+//   * random-triplet accuracy: the share of triplets (i, j, l) whose order "j closer to i than l"
+//     agrees between data and embedding (reference f32 squared distances).
+#include "engine.cuh"
+
+namespace pacmap {
+namespace {
+
+__global__ void overlap_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint64_t rows, int k,
+                               unsigned long long* __restrict__ hits) {
+  const uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  unsigned long long h = 0;
+  for (int p = 0; p < k; ++p) {
+    const uint32_t v = a[r * k + p];
+    for (int q = 0; q < k; ++q) h += (b[r * k + q] == v) ? 1ull : 0ull;
+  }
+  atomicAdd(hits, h);
+}
+
+__global__ void triplet_kernel(const float* __restrict__ xh, int d, const float* __restrict__ yl, int dim,
+                               const uint32_t* __restrict__ trip, uint64_t n_trip,
+                               unsigned long long* __restrict__ ok) {
+  const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  unsigned long long good = 0;
+  if (t < n_trip) {
+    const uint64_t i = trip[3 * t], j = trip[3 * t + 1], l = trip[3 * t + 2];
+    const float hj = ref_dist_sq(xh + i * d, xh + j * d, d), hl = ref_dist_sq(xh + i * d, xh + l * d, d);
+    const float sj = ref_dist_sq(yl + i * dim, yl + j * dim, dim), sl = ref_dist_sq(yl + i * dim, yl + l * dim, dim);
+    good = ((hj < hl) == (sj < sl)) ? 1ull : 0ull;
+  }
+  good = __reduce_add_sync(0xFFFFFFFFu, static_cast<unsigned>(good));
+  if ((threadIdx.x & 31) == 0 && good) atomicAdd(ok, good);
+}
+
+}  // namespace
+
+void quality_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, const float* d_y, uint64_t dim,
+                    const uint32_t* d_sample, uint64_t n_sample, uint64_t k, const uint32_t* d_trip, uint64_t n_trip,
+                    double* h_pres, double* h_trip) {
+  DevBuf<unsigned long long> counters(c, 2);
+  PM_CUDA(cudaMemsetAsync(counters.get(), 0, 2 * sizeof(unsigned long long), c.stream));
+  const uint64_t kq = std::min<uint64_t>(k, n > 0 ? n - 1 : 0);
+  if (n_sample > 0 && kq > 0) {
+    DevBuf<uint32_t> ih(c, n_sample * kq), il(c, n_sample * kq);
+    DevBuf<float> dh(c, n_sample * kq), dl(c, n_sample * kq);
+    knn_rows_simt(c, d_xp, n, d, kq, d_sample, n_sample, ih.get(), dh.get());
+    knn_rows_simt(c, d_y, n, dim, kq, d_sample, n_sample, il.get(), dl.get());
+    overlap_kernel<<<ceil_div(n_sample, 128), 128, 0, c.stream>>>(ih.get(), il.get(), n_sample, static_cast<int>(kq),
+                                                                 counters.get());
+    PM_LAUNCHED();
+  }
+  if (n_trip > 0) {
+    triplet_kernel<<<ceil_div(n_trip, 256), 256, 0, c.stream>>>(d_xp, static_cast<int>(d), d_y, static_cast<int>(dim),
+                                                               d_trip, n_trip, counters.get() + 1);
+    PM_LAUNCHED();
+  }
+  unsigned long long h[2];
+  PM_CUDA(cudaMemcpyAsync(h, counters.get(), sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+  PM_CUDA(cudaStreamSynchronize(c.stream));
+  if (h_pres) *h_pres = (n_sample && kq) ? static_cast<double>(h[0]) / static_cast<double>(n_sample * kq) : 0.0;
+  if (h_trip) *h_trip = n_trip ? static_cast<double>(h[1]) / static_cast<double>(n_trip) : 0.0;
+}
+
+}  // namespace pacmap

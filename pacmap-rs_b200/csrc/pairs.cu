@@ -1,0 +1,257 @@
+// Pair generation after the kNN -- src/neighbors.rs:56-108 and src/sampling.rs:37-313.
+//
+//   K4 sigma_kernel / reselect_kernel: sigma_i = mean(dist[i, 3..6]) floored at 1e-10
+//      (neighbors.rs:79-84), scaled = d*d / (sigma_i*sigma_j) (distance.rs:27-37), each row's k' scaled
+//      distances ordered by f32::total_cmp (ties: lower kNN column) and the first k kept
+//      (sampling.rs:251-286). One warp per row, bitonic sort in shared memory.
+//   K5 sample_fp_kernel: far pairs (sampling.rs:37-103): n_fp distinct partners per point, not the
+//      point, not among its k nearest neighbours, by rejection on the point's Philox stream.
+//   K6 sample_mn_kernel: mid-near pairs (sampling.rs:118-142, 296-313): per slot, 6 distinct
+//      candidates (not the point, not an earlier pick), the 2nd smallest reference f32 distance wins.
+//
+// Both samplers give one warp to one point: every lane replays the same Philox stream (no shuffles
+// for the draws), membership tests are split across lanes and combined with a ballot.
+#include "engine.cuh"
+
+namespace pacmap {
+namespace {
+
+__global__ void sigma_kernel(const float* __restrict__ kd, uint64_t n, int kp, float* __restrict__ sig) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int start = min(3, kp > 0 ? kp - 1 : 0);
+  const int end = min(6, kp);
+  if (end <= start) {
+    sig[i] = 1e-10f;
+    return;
+  }
+  float s = 0.0f;
+  for (int cc = start; cc < end; ++cc) s = __fadd_rn(s, kd[i * kp + cc]);
+  const float m = __fdiv_rn(s, static_cast<float>(end - start));
+  sig[i] = fmaxf(m, 1e-10f);
+}
+
+constexpr int RS_WARPS = 4;
+
+__global__ void __launch_bounds__(RS_WARPS * 32) reselect_kernel(const uint32_t* __restrict__ nbr,
+                                                                 const float* __restrict__ kd,
+                                                                 const float* __restrict__ sig, uint64_t n, int kp,
+                                                                 int k, int P, uint32_t* __restrict__ pnn) {
+  extern __shared__ uint64_t rs_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t* buf = rs_smem + warp * P;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * RS_WARPS + warp; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * RS_WARPS) {
+    const float si = sig[i];
+    for (int cc = lane; cc < P; cc += 32) {
+      uint64_t key = ~0ull;
+      if (cc < kp) {
+        const float dd = kd[i * kp + cc];
+        const float s = __fdiv_rn(__fmul_rn(dd, dd), __fmul_rn(si, sig[nbr[i * kp + cc]]));
+        key = (static_cast<uint64_t>(total_key(s)) << 32) | static_cast<uint32_t>(cc);
+      }
+      buf[cc] = key;
+    }
+    warp_bitonic_sort_u64(buf, P);
+    for (int j = lane; j < k; j += 32) {
+      const uint32_t cc = static_cast<uint32_t>(buf[j] & 0xFFFFFFFFu);
+      pnn[(i * k + j) * 2 + 0] = static_cast<uint32_t>(i);
+      pnn[(i * k + j) * 2 + 1] = nbr[i * kp + cc];
+    }
+    __syncwarp();
+  }
+}
+
+// True when any lane finds v among list[0 .. len) (stride `stride` elements).
+__device__ __forceinline__ bool warp_contains(const uint32_t* __restrict__ list, uint64_t stride, uint32_t len,
+                                              uint32_t v) {
+  bool hit = false;
+  for (uint32_t t = lane_id(); t < len; t += 32) hit |= (list[t * stride] == v);
+  return __any_sync(0xFFFFFFFFu, hit);
+}
+
+__global__ void sample_fp_kernel(const uint32_t* __restrict__ pnn, uint64_t n, uint32_t k, uint32_t n_fp,
+                                 uint64_t seed, uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  const uint32_t lane = lane_id();
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const uint32_t* reject = pnn + (i * k) * 2 + 1;  // column 1 of rows i*k .. (i+1)*k
+    uint32_t* picks = out + (i * n_fp) * 2 + 1;      // column 1 of this point's output rows
+    const bool self_in = warp_contains(reject, 2, k, static_cast<uint32_t>(i));
+    uint64_t avail = n > k ? n - k : 0;
+    const uint64_t self_cut = self_in ? 0 : 1;
+    avail = avail > self_cut ? avail - self_cut : 0;
+    const uint32_t want = static_cast<uint32_t>((n_fp < avail ? static_cast<uint64_t>(n_fp) : avail));
+    PointStream s(seed, i);
+    uint64_t budget = SAMPLE_ATTEMPT_CAP;
+    uint32_t cnt = 0;
+    while (cnt < want) {
+      uint32_t j;
+      if (!s.uniform(static_cast<uint32_t>(n), j, budget)) {
+        if (lane == 0) atomicOr(err, DEV_ERR_SAMPLING);
+        break;
+      }
+      if (j == i) continue;
+      if (warp_contains(picks, 2, cnt, j) || warp_contains(reject, 2, k, j)) continue;
+      if (lane == 0) {
+        out[(i * n_fp + cnt) * 2 + 0] = static_cast<uint32_t>(i);
+        out[(i * n_fp + cnt) * 2 + 1] = j;
+      }
+      __syncwarp();
+      ++cnt;
+    }
+  }
+}
+
+// The reference's f32 distance between rows a and b computed by an 8-lane group (l8 = lane % 8):
+// lane l8 forms the lane accumulator l8 of distance.rs:60-66, the group sums them in order 0..7,
+// adds the serial tail and takes the square root. Every lane of the group returns the result.
+__device__ __forceinline__ float group8_ref_dist(const float* __restrict__ a, const float* __restrict__ b, int d,
+                                                 int l8, unsigned group_base) {
+  float acc = 0.0f;
+  const int nc = d >> 3;
+  for (int ch = 0; ch < nc; ++ch) {
+    const float df = __fsub_rn(a[8 * ch + l8], b[8 * ch + l8]);
+    acc = __fadd_rn(acc, __fmul_rn(df, df));
+  }
+  float t = 0.0f;
+#pragma unroll
+  for (int l = 0; l < 8; ++l) t = __fadd_rn(t, __shfl_sync(0xFFFFFFFFu, acc, group_base + l));
+  for (int e = nc * 8; e < d; ++e) {
+    const float df = __fsub_rn(a[e], b[e]);
+    t = __fadd_rn(t, __fmul_rn(df, df));
+  }
+  return __fsqrt_rn(t);
+}
+
+__global__ void sample_mn_kernel(const float* __restrict__ x, uint64_t n, int d, uint32_t n_mn, uint64_t seed,
+                                 uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  const uint32_t lane = lane_id();
+  const int l8 = lane & 7;
+  const unsigned gbase = lane & ~7u;
+  const int grp = lane >> 3;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    uint32_t* picks = out + (i * n_mn) * 2 + 1;
+    PointStream s(seed, i);
+    uint64_t budget = SAMPLE_ATTEMPT_CAP;
+    bool failed = false;
+    for (uint32_t jslot = 0; jslot < n_mn && !failed; ++jslot) {
+      const bool self_in = warp_contains(picks, 2, jslot, static_cast<uint32_t>(i));
+      uint64_t avail = n > jslot ? n - jslot : 0;
+      const uint64_t self_cut = self_in ? 0 : 1;
+      avail = avail > self_cut ? avail - self_cut : 0;
+      const uint32_t want = static_cast<uint32_t>((avail < 6 ? avail : 6ull));
+      uint32_t cand[6] = {0, 0, 0, 0, 0, 0};
+      uint32_t cnt = 0;
+      while (cnt < want) {
+        uint32_t j;
+        if (!s.uniform(static_cast<uint32_t>(n), j, budget)) {
+          failed = true;
+          break;
+        }
+        if (j == i) continue;
+        bool dup = false;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) dup |= (t < static_cast<int>(cnt) && cand[t] == j);
+        if (dup || warp_contains(picks, 2, jslot, j)) continue;
+#pragma unroll
+        for (int t = 0; t < 6; ++t)
+          if (t == static_cast<int>(cnt)) cand[t] = j;
+        ++cnt;
+      }
+      if (failed) {
+        if (lane == 0) atomicOr(err, DEV_ERR_SAMPLING);
+        break;
+      }
+      // Distances of the drawn candidates: group g (lanes 8g..8g+7) handles slots g and g + 4.
+      float dist[6];
+#pragma unroll
+      for (int pass = 0; pass < 2; ++pass) {
+        const int slot = pass * 4 + grp;
+        float dv = 0.0f;
+        uint32_t cidx = 0;
+#pragma unroll
+        for (int t = 0; t < 6; ++t)
+          if (t == slot) cidx = cand[t];
+        const bool active = slot < static_cast<int>(cnt);
+        // Groups with nothing to do still join the shuffles inside group8_ref_dist (on row i itself).
+        const float r = group8_ref_dist(x + i * d, x + static_cast<uint64_t>(active ? cidx : i) * d, d, l8, gbase);
+        dv = active ? r : 0.0f;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const float v = __shfl_sync(0xFFFFFFFFu, dv, g * 8);
+          if (pass * 4 + g < 6) dist[pass * 4 + g] = v;
+        }
+      }
+      // Slots >= cnt are the reference's (0.0, 0) fill. Pick the 2nd smallest (key, slot).
+      uint64_t best0 = ~0ull, best1 = ~0ull;
+      uint32_t id0 = 0, id1 = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const bool real = t < static_cast<int>(cnt);
+        const float dv = real ? dist[t] : 0.0f;
+        const uint32_t id = real ? cand[t] : 0u;
+        const uint64_t key = (static_cast<uint64_t>(total_key(dv)) << 3) | static_cast<uint64_t>(t);
+        if (key < best0) {
+          best1 = best0;
+          id1 = id0;
+          best0 = key;
+          id0 = id;
+        } else if (key < best1) {
+          best1 = key;
+          id1 = id;
+        }
+      }
+      if (lane == 0) {
+        out[(i * n_mn + jslot) * 2 + 0] = static_cast<uint32_t>(i);
+        out[(i * n_mn + jslot) * 2 + 1] = id1;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+}  // namespace
+
+void sigma_device(Ctx& c, const float* d_kd, uint64_t n, uint64_t kp, float* d_sig) {
+  sigma_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(d_kd, n, static_cast<int>(kp), d_sig);
+  PM_LAUNCHED();
+}
+
+void reselect_device(Ctx& c, const uint32_t* d_nbr, const float* d_kd, const float* d_sig, uint64_t n, uint64_t kp,
+                     uint64_t k, uint32_t* d_pnn) {
+  if (n == 0 || k == 0) return;
+  PM_REQUIRE(kp <= 4096 && k <= kp, PACMAP_ERR_UNSUPPORTED, "neighbour reselection supports k' <= 4096");
+  const int P = next_pow2(static_cast<int>(kp));
+  const size_t smem = static_cast<size_t>(RS_WARPS) * P * sizeof(uint64_t);
+  PM_CUDA(cudaFuncSetAttribute(reselect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n, RS_WARPS), c.sm_count * 16ull));
+  reselect_kernel<<<grid, RS_WARPS * 32, smem, c.stream>>>(d_nbr, d_kd, d_sig, n, static_cast<int>(kp),
+                                                           static_cast<int>(k), P, d_pnn);
+  PM_LAUNCHED();
+}
+
+void sample_fp_device(Ctx& c, const uint32_t* d_pnn, uint64_t n, uint64_t k, uint64_t n_fp, uint64_t seed,
+                      uint32_t* d_pfp) {
+  if (n == 0 || n_fp == 0) return;
+  PM_REQUIRE(n < (1ull << 32), PACMAP_ERR_UNSUPPORTED, "pair indices are u32: n must be < 2^32");
+  PM_CUDA(cudaMemsetAsync(d_pfp, 0, n * n_fp * 2 * sizeof(uint32_t), c.stream));
+  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n, 8), c.sm_count * 32ull));
+  sample_fp_kernel<<<grid, 256, 0, c.stream>>>(d_pnn, n, static_cast<uint32_t>(k), static_cast<uint32_t>(n_fp), seed,
+                                               d_pfp, c.d_err);
+  PM_LAUNCHED();
+}
+
+void sample_mn_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, uint64_t n_mn, uint64_t seed,
+                      uint32_t* d_pmn) {
+  if (n == 0 || n_mn == 0) return;
+  PM_REQUIRE(n < (1ull << 32), PACMAP_ERR_UNSUPPORTED, "pair indices are u32: n must be < 2^32");
+  PM_CUDA(cudaMemsetAsync(d_pmn, 0, n * n_mn * 2 * sizeof(uint32_t), c.stream));
+  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n, 8), c.sm_count * 32ull));
+  sample_mn_kernel<<<grid, 256, 0, c.stream>>>(d_xp, n, static_cast<int>(d), static_cast<uint32_t>(n_mn), seed,
+                                               d_pmn, c.d_err);
+  PM_LAUNCHED();
+}
+
+}  // namespace pacmap
