@@ -188,7 +188,9 @@ pacmap_status pacmap_quality(const float* x, uint64_t n, uint64_t d, const float
 
 /* Stage timing (diagnostics): when enabled, each fit_transform records the device time of its stages
  * with CUDA events on its stream. pacmap_stage_times fills up to `cap` values in milliseconds, in the
- * order preprocess, knn, reselect, sample_mn, sample_fp, csr, init, optimize, and returns how many. */
+ * order preprocess, knn, reselect, sample_mn, sample_fp, csr, init, optimize (then, when the tensor-core
+ * kNN ran: its filter kernel alone, and the number of rows it left to the exact fallback), and returns
+ * how many. */
 void pacmap_set_stage_timing(int32_t enabled);
 uint64_t pacmap_stage_times(double* out_ms, uint64_t cap);
 

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "engine.cuh"
+#include "knn_tc.cuh"
 
 namespace pacmap {
 
@@ -152,7 +153,7 @@ struct StageTimer {
   explicit StageTimer(cudaStream_t stream) : s(stream), on(g_stage_timing) {
     if (!on) return;
     for (auto& e : ev) PM_CUDA(cudaEventCreate(&e));
-    g_stage_ms.assign(ST_COUNT, 0.0);
+    g_stage_ms.assign(ST_COUNT, 0.0);  // + knn_filter ms and fallback rows appended by the kNN stage
   }
   void start(int stage) {
     if (on) PM_CUDA(cudaEventRecord(ev[stage], s));
@@ -184,8 +185,15 @@ void generate_pairs_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, co
   DevBuf<uint32_t> idx(c, n * kp);
   DevBuf<float> dist(c, n * kp), sig(c, n);
   if (tm) tm->start(ST_KNN);
+  last_tc_filter_ms() = 0.0;
+  last_tc_fallback_rows() = 0;
   knn_exact_device(c, d_xp, n, d, kp, knn_mode, idx.get(), dist.get());
   if (tm) tm->stop(ST_KNN);
+  if (tm && tm->on) {
+    g_stage_ms.resize(ST_COUNT + 2, 0.0);
+    g_stage_ms[ST_COUNT] = last_tc_filter_ms();
+    g_stage_ms[ST_COUNT + 1] = static_cast<double>(last_tc_fallback_rows());
+  }
   if (tm) tm->start(ST_RESELECT);
   sigma_device(c, dist.get(), n, kp, sig.get());
   out.nn.alloc(c, n * k * 2);

@@ -66,8 +66,9 @@ void column_mean_seq(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float sub
 void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, int mode, uint32_t* d_idx,
                       float* d_dist);
 // Exact kNN of a subset of rows (query ids in d_rows) against all rows.
+// scatter: results go to the rows' own places (row r -> d_idx[r * kp]) instead of list order.
 void knn_rows_simt(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, const uint32_t* d_rows,
-                   uint64_t n_rows, uint32_t* d_idx, float* d_dist);
+                   uint64_t n_rows, uint32_t* d_idx, float* d_dist, bool scatter = false);
 
 // ---- pairs.cu ----
 void sigma_device(Ctx& c, const float* d_kd, uint64_t n, uint64_t kp, float* d_sig);

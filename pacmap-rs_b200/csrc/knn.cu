@@ -26,7 +26,7 @@ constexpr int SQ_MAX_K = 448;     // P = next_pow2(K + KT) <= 512
 __global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __restrict__ x, uint64_t n, int d, int K,
                                                               int P, const uint32_t* __restrict__ rows,
                                                               uint64_t n_rows, uint32_t* __restrict__ out_idx,
-                                                              float* __restrict__ out_dist) {
+                                                              float* __restrict__ out_dist, int scatter) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* qs = reinterpret_cast<float*>(smem);
   float* ks = qs + SQ_QB * SQ_LD;
@@ -133,15 +133,16 @@ __global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __res
     const uint64_t s = slot0 + qi;
     if (s >= n_rows) continue;
     const uint64_t key = lists[qi * P + cc];
-    out_idx[s * K + cc] = static_cast<uint32_t>(key & 0xFFFFFFFFu);
-    out_dist[s * K + cc] = key_to_float(static_cast<uint32_t>(key >> 32));
+    const uint64_t o = scatter ? qrow[qi] : s;
+    out_idx[o * K + cc] = static_cast<uint32_t>(key & 0xFFFFFFFFu);
+    out_dist[o * K + cc] = key_to_float(static_cast<uint32_t>(key >> 32));
   }
 }
 
 }  // namespace
 
 void knn_rows_simt(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, const uint32_t* d_rows,
-                   uint64_t n_rows, uint32_t* d_idx, float* d_dist) {
+                   uint64_t n_rows, uint32_t* d_idx, float* d_dist, bool scatter) {
   if (n_rows == 0 || kp == 0) return;
   PM_REQUIRE(kp <= SQ_MAX_K, PACMAP_ERR_UNSUPPORTED,
              "exact kNN supports at most " + std::to_string(SQ_MAX_K) + " neighbours per row");
@@ -151,14 +152,17 @@ void knn_rows_simt(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   const size_t smem = static_cast<size_t>(SQ_QB + SQ_KT) * SQ_LD * sizeof(float) + static_cast<size_t>(SQ_QB) * P * 8;
   PM_CUDA(cudaFuncSetAttribute(knn_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   knn_simt_kernel<<<ceil_div(n_rows, SQ_QB), SQ_THREADS, smem, c.stream>>>(d_x, n, static_cast<int>(d), K, P, d_rows,
-                                                                         n_rows, d_idx, d_dist);
+                                                                         n_rows, d_idx, d_dist, scatter ? 1 : 0);
   PM_LAUNCHED();
 }
 
 void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, int mode, uint32_t* d_idx,
                       float* d_dist) {
   if (n == 0 || kp == 0) return;
-  if (mode != PACMAP_KNN_SIMT_EXACT && knn_tc_supported(n, d, kp)) {
+  // AUTO uses the tensor cores once the O(n^2) part dominates; the TENSOR modes force them.
+  const bool want_tc = (mode == PACMAP_KNN_TENSOR_F16 || mode == PACMAP_KNN_TENSOR_BF16) ||
+                       (mode == PACMAP_KNN_AUTO && n >= 16384);
+  if (want_tc && knn_tc_supported(n, d, kp)) {
     if (knn_tc_device(c, d_x, n, d, kp, mode == PACMAP_KNN_TENSOR_BF16, d_idx, d_dist)) return;
   }
   PM_REQUIRE(mode == PACMAP_KNN_AUTO || mode == PACMAP_KNN_SIMT_EXACT, PACMAP_ERR_UNSUPPORTED,

@@ -1,7 +1,791 @@
-// Tensor-core (tcgen05) distance-GEMM filter for the exact kNN.
+// Exact kNN through a tensor-core filter (tcgen05 + TMA + TMEM) and an exact FP32 re-rank.
+//
+// The reference ranks neighbours by its f32 distance (src/knn.rs:149-191, src/distance.rs:50-75). Here
+// the O(n^2 d) part runs as a distance GEMM on the 5th-generation tensor cores and only a small,
+// provably complete candidate set per row is re-ranked with the reference's exact f32 arithmetic:
+//
+//  1. prep: x is scaled by an exact power of two s (max |x s| < 2^13), split into h = fp16(x s) (or
+//     bf16) and l = x s - h; per point n = ||x s||^2, A = ||h||^2, B = ||l||^2 (f32).
+//  2. knn_filter_kernel: per 256-row block, G = h_i . h_j for every column tile of 128 points by
+//     tcgen05.mma (M=128 x2 halves, N=128, K=16 steps, FP32 accumulators in TMEM, operands staged by
+//     TMA with 128-byte swizzle). The epilogue forms v_ij = (n_j - 2 e_j) - 2 G_ij.
+//     Error bound: with e_j = (rho A_j + B_j / rho)/2 + B_j/2 + eta A_j/2 + gamma n_j (AM-GM on the
+//     Cauchy-Schwarz bound of h.l + l.h + l.l, eta = tensor-core accumulation, gamma = every f32
+//     rounding incl. the reference's own distance sum), the reference's squared distance lies in
+//     [LB, UB] = [v + n_i - 2e_i, v + 4e_j + n_i + 2e_i].
+//     Each row keeps a buffer of candidates with v <= theta_i, where theta_i comes from the (k'+1)-th
+//     smallest UB seen so far (the +1 covers the row itself); when the buffer fills, the owning warp
+//     compacts it with a radix select. Any true neighbour has LB <= k'-th UB, so it is never dropped.
+//  3. knn_rerank_kernel: the final threshold, then the reference's exact f32 distance of every
+//     survivor, sorted by (distance, index): the rows of knn.rs.
+//  Rows whose candidate band does not fit the buffer (e.g. thousands of exact duplicates) are
+//  recomputed by the exact SIMT kernel.
+//
+// Every mbarrier wait is bounded (2 s of %globaltimer): a kernel that gives up raises DEV_ERR_TIMEOUT
+// and returns after releasing its tensor memory. No TMA multicast is used anywhere.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "knn_tc.cuh"
 
 namespace pacmap {
-bool knn_tc_supported(uint64_t, uint64_t, uint64_t) { return false; }
-bool knn_tc_device(Ctx&, const float*, uint64_t, uint64_t, uint64_t, bool, uint32_t*, float*) { return false; }
+
+namespace {
+
+constexpr int TC_BM = 256;         // rows per block (two M = 128 accumulators)
+constexpr int TC_BN = 128;         // columns per tile (MMA N)
+constexpr int TC_STAGES = 4;       // B-operand pipeline depth
+constexpr int TC_THREADS = 320;    // warp 0 TMA, warp 1 MMA + TMEM owner, warps 2..9 epilogue
+constexpr int TC_EPI_WARPS = 8;
+constexpr int TC_TMEM_COLS = 512;  // 2 accumulator stages x 2 halves x 128 columns
+constexpr int KB_BYTES = 128 * 128;  // one 128-row x 64-element (128 B) swizzled K block
+
+struct alignas(8) TcShared {
+  uint64_t full[TC_STAGES];
+  uint64_t empty[TC_STAGES];
+  uint64_t a_full;
+  uint64_t tmem_full[2];
+  uint64_t tmem_empty[2];
+  uint64_t mma_done;
+  uint32_t tmem_base;
+  int abort_flag;
+  uint32_t hist[TC_EPI_WARPS][256];
+};
+
+// ---------------------------------------------------------------------------------------------
+// PTX wrappers (sm_100a).
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s: far above any legitimate wait here
+
+// Bounded wait on a barrier phase; false when it gave up (timeout, or another role aborted).
+__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 63) == 0) {
+      if (*abort_flag) return false;
+      if (globaltimer() - t0 > WAIT_LIMIT_NS) return false;
+    }
+  }
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128-byte-swizzled shared-memory matrix descriptor (tcgen05 "matrix descriptor"):
+// start address >> 4, leading offset 16 B (unused for swizzled K-major), stride offset 1024 B between
+// 8-row core groups, descriptor version 1, swizzle mode 2 (128 B).
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
+  uint64_t d = static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
+  d |= static_cast<uint64_t>(1) << 16;
+  d |= static_cast<uint64_t>(1024 >> 4) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(2) << 61;
+  return d;
+}
+// Instruction descriptor, kind::f16: D f32, A/B f16 (0) or bf16 (1), both K-major, N = 128, M = 128.
+__host__ __device__ constexpr uint32_t idesc_f16(bool bf16) {
+  return (1u << 4) | ((bf16 ? 1u : 0u) << 7) | ((bf16 ? 1u : 0u) << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+}
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::
+          "r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Per-row candidate buffer maintenance (shared by the filter's compaction and the re-rank).
+// ---------------------------------------------------------------------------------------------
+
+// Rank-`rank` (1-based) smallest of total_key(u[0..m)) by a 4-pass 8-bit radix select, one warp.
+__device__ __forceinline__ uint32_t warp_radix_select(const float* __restrict__ u, int m, int rank, uint32_t* hist) {
+  const int lane = threadIdx.x & 31;
+  uint32_t prefix = 0, mask = 0;
+  int need = rank;
+#pragma unroll 1
+  for (int pass = 0; pass < 4; ++pass) {
+    const int shift = 24 - 8 * pass;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) hist[lane * 8 + b] = 0;
+    __syncwarp();
+    for (int e = lane; e < m; e += 32) {
+      const uint32_t key = total_key(u[e]);
+      if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+    }
+    __syncwarp();
+    uint32_t local[8], lsum = 0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      local[b] = hist[lane * 8 + b];
+      lsum += local[b];
+    }
+    uint32_t incl = lsum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const uint32_t excl = incl - lsum;
+    // the lane whose bins contain the `need`-th element
+    const bool mine = (excl < static_cast<uint32_t>(need)) && (static_cast<uint32_t>(need) <= incl);
+    const unsigned who = __ballot_sync(0xFFFFFFFFu, mine);
+    const int src = who ? (__ffs(who) - 1) : 31;
+    int bin = 0;
+    uint32_t before = 0;
+    if (mine) {
+      uint32_t run = excl;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        if (run + local[b] >= static_cast<uint32_t>(need)) {
+          bin = lane * 8 + b;
+          before = run;
+          break;
+        }
+        run += local[b];
+      }
+    }
+    bin = __shfl_sync(0xFFFFFFFFu, bin, src);
+    before = __shfl_sync(0xFFFFFFFFu, before, src);
+    prefix |= static_cast<uint32_t>(bin) << shift;
+    mask |= 255u << shift;
+    need -= static_cast<int>(before);
+    __syncwarp();
+  }
+  return prefix;
+}
+
+// theta for row constants (n_i, e4_i = 4 e_i) and the selected UB key: v <= theta keeps every
+// candidate whose lower bound is within the (sqrt-tie-widened) k'-th upper bound.
+__device__ __forceinline__ float theta_from(uint32_t ukey, float n_i, float e4_i) {
+  const float uT = key_to_float(ukey);
+  const float base = uT + e4_i;
+  const float slack = 9.5367431640625e-07f * fabsf(uT + n_i + 0.5f * e4_i) + 2.384185791015625e-07f * (n_i + fabsf(uT));
+  return base + slack;
+}
+
+// Keeps entries with v <= theta, preserving order; returns the new count. One warp.
+__device__ __forceinline__ int warp_compact(uint32_t* __restrict__ idx, float* __restrict__ v, float* __restrict__ u,
+                                            int m, float theta) {
+  const int lane = threadIdx.x & 31;
+  int out = 0;
+  for (int e0 = 0; e0 < m; e0 += 32) {
+    const int e = e0 + lane;
+    uint32_t ii = 0;
+    float vv = 0.0f, uu = 0.0f;
+    bool keep = false;
+    if (e < m) {
+      vv = v[e];
+      keep = vv <= theta;
+      if (keep) {
+        ii = idx[e];
+        uu = u[e];
+      }
+    }
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
+    __syncwarp();
+    if (keep) {
+      const int pos = out + __popc(bal & ((1u << lane) - 1u));
+      idx[pos] = ii;
+      v[pos] = vv;
+      u[pos] = uu;
+    }
+    out += __popc(bal);
+    __syncwarp();
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------------------------
+// 1. prep
+// ---------------------------------------------------------------------------------------------
+__global__ void absmax_kernel(const float* __restrict__ x, uint64_t total, uint32_t* __restrict__ out) {
+  uint32_t m = 0;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const float a = fabsf(x[t]);
+    if (a == a) m = max(m, __float_as_uint(a));  // NaN excluded
+  }
+  m = __reduce_max_sync(0xFFFFFFFFu, m);
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+template <bool BF16>
+__global__ void split_rows_kernel(const float* __restrict__ x, uint64_t n, int d, int KP, uint64_t n_pad, float s,
+                                  uint16_t* __restrict__ H, float* __restrict__ nrm, float* __restrict__ A,
+                                  float* __restrict__ B, double* __restrict__ partial) {
+  __shared__ double red[2][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double sa = 0.0, sb = 0.0;
+  for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * 8 + warp; r < n_pad; r += static_cast<uint64_t>(gridDim.x) * 8) {
+    float nn = 0.0f, aa = 0.0f, bb = 0.0f;
+    for (int c = lane; c < KP; c += 32) {
+      float xs = 0.0f;
+      if (r < n && c < d) xs = x[r * d + c] * s;
+      uint16_t hbits;
+      float hf;
+      if (BF16) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(xs);
+        hbits = __bfloat16_as_ushort(h);
+        hf = __bfloat162float(h);
+      } else {
+        const __half h = __float2half_rn(xs);
+        hbits = __half_as_ushort(h);
+        hf = __half2float(h);
+      }
+      const float l = xs - hf;
+      H[r * KP + c] = hbits;
+      nn = fmaf(xs, xs, nn);
+      aa = fmaf(hf, hf, aa);
+      bb = fmaf(l, l, bb);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      nn += __shfl_xor_sync(0xFFFFFFFFu, nn, o);
+      aa += __shfl_xor_sync(0xFFFFFFFFu, aa, o);
+      bb += __shfl_xor_sync(0xFFFFFFFFu, bb, o);
+    }
+    if (lane == 0 && r < n) {
+      nrm[r] = nn;
+      A[r] = aa;
+      B[r] = bb;
+      sa += aa;
+      sb += bb;
+    }
+  }
+  if (lane == 0) {
+    red[0][warp] = sa;
+    red[1][warp] = sb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      ta += red[0][w];
+      tb += red[1][w];
+    }
+    partial[2 * blockIdx.x] = ta;
+    partial[2 * blockIdx.x + 1] = tb;
+  }
+}
+
+// e_j and the per-column/per-row constants of the filter. Slack factors: the f32 sums of n, A, B
+// are inflated by 2^-16 relative; gamma covers the reference's own f32 distance sum, every f32
+// rounding of the epilogue and of these constants.
+__global__ void bound_kernel(uint64_t n, uint64_t n_pad, int d, int KP, float rho, const float* __restrict__ nrm,
+                             const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ g,
+                             float* __restrict__ e4) {
+  const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (j >= n_pad) return;
+  if (j >= n) {
+    g[j] = __int_as_float(0x7f800000);  // +inf: padding columns never pass
+    e4[j] = 0.0f;
+    return;
+  }
+  const float infl = 1.0f + 1.52587890625e-05f;  // 1 + 2^-16
+  const float a = A[j] * infl, b = B[j] * infl, nn = nrm[j] * infl;
+  const float eta = static_cast<float>(KP) * 4.76837158203125e-07f;                   // K * 2^-21
+  // f32 sums of n (d terms), the reference's own distance sum (d/8 + 8 terms, on D <= 2(n_i + n_j)),
+  // and the epilogue's roundings: (2d + 64) 2^-24 + 2^-19.
+  const float gamma = static_cast<float>(2 * d + 64) * 5.9604644775390625e-08f + 1.9073486328125e-06f;
+  const float e = 0.5f * (rho * a + b / rho) + 0.5f * b + 0.5f * eta * a + gamma * nn + 1e-30f;
+  const float e_safe = e * (1.0f + 9.765625e-04f);  // 2^-10 relative margin on the bound itself
+  g[j] = nrm[j] - 2.0f * e_safe;
+  e4[j] = 4.0f * e_safe;
+}
+
+// ---------------------------------------------------------------------------------------------
+// 2. the tcgen05 filter
+// ---------------------------------------------------------------------------------------------
+template <int KB>  // K blocks of 64 elements: KP = 64 * KB
+__global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
+    const __grid_constant__ CUtensorMap hmap, uint64_t n, uint64_t n_pad, uint32_t idesc, const float* __restrict__ g,
+    const float* __restrict__ e4, const float* __restrict__ nrm, int C, int rank, uint32_t* __restrict__ cand_idx,
+    float* __restrict__ cand_v, float* __restrict__ cand_u, int* __restrict__ cand_cnt, uint32_t* __restrict__ overflow_rows,
+    uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  // 1024-byte aligned operand region: A [2 halves][KB][16 KB], B [STAGES][KB][16 KB], then TcShared.
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* a_smem = base;
+  unsigned char* b_smem = base + 2 * KB * KB_BYTES;
+  TcShared* sh = reinterpret_cast<TcShared*>(b_smem + TC_STAGES * KB * KB_BYTES);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t row0 = static_cast<uint64_t>(blockIdx.x) * TC_BM;
+  const int ntiles = static_cast<int>(n_pad / TC_BN);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TC_STAGES; ++s) {
+      mbar_init(&sh->full[s], 1);
+      mbar_init(&sh->empty[s], 1);
+    }
+    mbar_init(&sh->a_full, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&sh->tmem_full[a], 1);
+      mbar_init(&sh->tmem_empty[a], TC_EPI_WARPS);
+    }
+    mbar_init(&sh->mma_done, 1);
+    sh->abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem_base)),
+                 "r"(TC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh->tmem_base;
+  volatile int* abort_flag = &sh->abort_flag;
+
+  if (warp == 0) {
+    // ------------------------------- TMA producer -------------------------------
+    if (lane == 0) {
+      mbar_expect_tx(&sh->a_full, 2 * KB * KB_BYTES);
+      for (int h = 0; h < 2; ++h)
+        for (int kb = 0; kb < KB; ++kb)
+          tma_load_2d(a_smem + (h * KB + kb) * KB_BYTES, &hmap, &sh->a_full, kb * 64, static_cast<int>(row0 + h * 128));
+      int issued = 0;
+      for (int t = 0; t < ntiles; ++t) {
+        const int s = t % TC_STAGES;
+        if (t >= TC_STAGES && !mbar_wait(&sh->empty[s], ((t / TC_STAGES) + 1) & 1, abort_flag)) break;
+        mbar_expect_tx(&sh->full[s], KB * KB_BYTES);
+        for (int kb = 0; kb < KB; ++kb)
+          tma_load_2d(b_smem + (s * KB + kb) * KB_BYTES, &hmap, &sh->full[s], kb * 64, t * TC_BN);
+        issued = t + 1;
+      }
+      if (issued < ntiles) {
+        atomicOr(err, DEV_ERR_TIMEOUT);
+        sh->abort_flag = 1;
+      }
+      // Drain: every issued load has landed before the block may exit.
+      mbar_wait(&sh->a_full, 0, abort_flag);
+      for (int t = (issued > TC_STAGES ? issued - TC_STAGES : 0); t < issued; ++t) {
+        const uint64_t t0 = globaltimer();
+        while (!mbar_try_wait(&sh->full[t % TC_STAGES], (t / TC_STAGES) & 1) && globaltimer() - t0 < WAIT_LIMIT_NS) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------- MMA issuer -------------------------------
+    if (lane == 0) {
+      bool ok = mbar_wait(&sh->a_full, 0, abort_flag);
+      const uint32_t a_addr = smem_u32(a_smem), b_addr = smem_u32(b_smem);
+      int t = 0;
+      for (; ok && t < ntiles; ++t) {
+        const int s = t % TC_STAGES, acc = t & 1;
+        if (!mbar_wait(&sh->full[s], (t / TC_STAGES) & 1, abort_flag)) {
+          ok = false;
+          break;
+        }
+        if (t >= 2 && !mbar_wait(&sh->tmem_empty[acc], ((t >> 1) + 1) & 1, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t d_tmem = tmem + acc * 256 + h * 128;
+#pragma unroll
+          for (int kb = 0; kb < KB; ++kb) {
+            const uint64_t ad = sdesc_sw128(a_addr + (h * KB + kb) * KB_BYTES);
+            const uint64_t bd = sdesc_sw128(b_addr + (s * KB + kb) * KB_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+              umma_f16(d_tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) ? 1u : 0u);
+          }
+        }
+        umma_commit(&sh->empty[s]);
+        umma_commit(&sh->tmem_full[acc]);
+      }
+      if (!ok) {
+        atomicOr(err, DEV_ERR_TIMEOUT);
+        sh->abort_flag = 1;
+      }
+      // Every issued MMA has completed before the tensor memory is released.
+      umma_commit(&sh->mma_done);
+      const uint64_t t0 = globaltimer();
+      while (!mbar_try_wait(&sh->mma_done, 0) && globaltimer() - t0 < WAIT_LIMIT_NS) {
+      }
+    }
+  } else {
+    // ------------------------------- epilogue (8 warps) -------------------------------
+    const int ew = warp - 2;
+    const int half = ew >> 2;
+    const int quad = warp & 3;  // TMEM lane quadrant this warp may access
+    const uint64_t row = row0 + half * 128 + quad * 32 + lane;
+    const bool valid = row < n;
+    uint32_t* hist = sh->hist[ew];
+    float theta = valid ? 3.402823466e+38f : -__int_as_float(0x7f800000);
+    int cnt = 0;
+    const float n_i = valid ? nrm[row] : 0.0f;
+    const float e4_i = valid ? e4[row] : 0.0f;
+    const uint64_t cbase = row * static_cast<uint64_t>(C);
+    bool ok = true;
+    for (int t = 0; t < ntiles; ++t) {
+      const int acc = t & 1;
+      if (!mbar_wait(&sh->tmem_full[acc], (t >> 1) & 1, abort_flag)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int col0 = t * TC_BN;
+      const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) + acc * 256 + half * 128;
+#pragma unroll 1
+      for (int ch = 0; ch < 4; ++ch) {
+        float G[32];
+        tmem_ld32(taddr + ch * 32, G);
+        const float4* gp = reinterpret_cast<const float4*>(g + col0 + ch * 32);
+        float v[32];
+        float vmin = __int_as_float(0x7f800000);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float4 gv = __ldg(gp + q);
+          v[4 * q + 0] = fmaf(-2.0f, G[4 * q + 0], gv.x);
+          v[4 * q + 1] = fmaf(-2.0f, G[4 * q + 1], gv.y);
+          v[4 * q + 2] = fmaf(-2.0f, G[4 * q + 2], gv.z);
+          v[4 * q + 3] = fmaf(-2.0f, G[4 * q + 3], gv.w);
+          vmin = fminf(vmin, fminf(fminf(v[4 * q + 0], v[4 * q + 1]), fminf(v[4 * q + 2], v[4 * q + 3])));
+        }
+        if (vmin <= theta) {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) {
+            if (v[c] <= theta) {
+              const uint32_t j = static_cast<uint32_t>(col0 + ch * 32 + c);
+              cand_idx[cbase + cnt] = j;
+              cand_v[cbase + cnt] = v[c];
+              cand_u[cbase + cnt] = v[c] + __ldg(e4 + j);
+              ++cnt;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh->tmem_empty[acc]);
+      // Compact full buffers so that the next tile (<= 128 insertions) always fits.
+      unsigned need = __ballot_sync(0xFFFFFFFFu, cnt > C - TC_BN);
+      while (need) {
+        const int L = __ffs(need) - 1;
+        need &= need - 1;
+        const uint64_t rb = __shfl_sync(0xFFFFFFFFu, cbase, L);
+        const int m = __shfl_sync(0xFFFFFFFFu, cnt, L);
+        const float nL = __shfl_sync(0xFFFFFFFFu, n_i, L);
+        const float eL = __shfl_sync(0xFFFFFFFFu, e4_i, L);
+        const uint32_t key = warp_radix_select(cand_u + rb, m, min(rank, m), hist);
+        const float th = theta_from(key, nL, eL);
+        __threadfence_block();
+        const int kept = warp_compact(cand_idx + rb, cand_v + rb, cand_u + rb, m, th);
+        if (lane == L) {
+          theta = th;
+          cnt = kept;
+          if (cnt > C - TC_BN) {  // the band does not fit: exact recomputation later
+            theta = -__int_as_float(0x7f800000);
+            cnt = 0;
+            overflow_rows[atomicAdd(n_overflow, 1u)] = static_cast<uint32_t>(row);
+          }
+        }
+        __syncwarp();
+      }
+    }
+    if (!ok) {
+      atomicOr(err, DEV_ERR_TIMEOUT);
+      sh->abort_flag = 1;
+    }
+    if (valid) cand_cnt[row] = (theta == -__int_as_float(0x7f800000)) ? -1 : cnt;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// 3. exact re-rank: one warp per row.
+// ---------------------------------------------------------------------------------------------
+constexpr int RR_WARPS = 4;
+
+__global__ void __launch_bounds__(RR_WARPS * 32) knn_rerank_kernel(
+    const float* __restrict__ x, uint64_t n, int d, int K, int C, int rank, const float* __restrict__ nrm,
+    const float* __restrict__ e4, uint32_t* __restrict__ cand_idx, float* __restrict__ cand_v,
+    float* __restrict__ cand_u, const int* __restrict__ cand_cnt, uint32_t* __restrict__ out_idx,
+    float* __restrict__ out_dist, uint32_t* __restrict__ fallback_rows, uint32_t* __restrict__ n_fallback) {
+  extern __shared__ uint64_t rr_smem[];
+  __shared__ uint32_t hist_all[RR_WARPS][256];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int P = next_pow2(C);
+  uint64_t* keys = rr_smem + warp * P;
+  uint32_t* hist = hist_all[warp];
+  const int l8 = lane & 7, grp = lane >> 3;
+  for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * RR_WARPS + warp; r < n;
+       r += static_cast<uint64_t>(gridDim.x) * RR_WARPS) {
+    const int m0 = min(cand_cnt[r], C);
+    if (m0 < 0) continue;  // overflowed in the filter: handled by the exact fallback
+    const uint64_t rb = r * static_cast<uint64_t>(C);
+    int m = m0;
+    if (m > 0) {
+      const uint32_t key = warp_radix_select(cand_u + rb, m, min(rank, m), hist);
+      const float th = theta_from(key, nrm[r], e4[r]);
+      m = warp_compact(cand_idx + rb, cand_v + rb, cand_u + rb, m, th);
+    }
+    // exact reference distances of the survivors (self excluded), 4 at a time per warp
+    int nk = 0;
+    for (int e0 = 0; e0 < m; e0 += 4) {
+      const int e = e0 + grp;
+      const uint32_t j = (e < m) ? cand_idx[rb + e] : static_cast<uint32_t>(r);
+      const float* a = x + r * d;
+      const float* b = x + static_cast<uint64_t>(j) * d;
+      float accl = 0.0f;
+      const int nc = d >> 3;
+      for (int ch = 0; ch < nc; ++ch) {
+        const float df = __fsub_rn(a[8 * ch + l8], b[8 * ch + l8]);
+        accl = __fadd_rn(accl, __fmul_rn(df, df));
+      }
+      float t = 0.0f;
+#pragma unroll
+      for (int l = 0; l < 8; ++l) t = __fadd_rn(t, __shfl_sync(0xFFFFFFFFu, accl, (lane & ~7) + l));
+      for (int q = nc * 8; q < d; ++q) {
+        const float df = __fsub_rn(a[q], b[q]);
+        t = __fadd_rn(t, __fmul_rn(df, df));
+      }
+      const float dist = __fsqrt_rn(t);
+      const bool real = (e < m) && (j != r);
+      const unsigned bal = __ballot_sync(0xFFFFFFFFu, real && l8 == 0);
+      if (real && l8 == 0) {
+        const int pos = nk + __popc(bal & ((1u << lane) - 1u));
+        keys[pos] = (static_cast<uint64_t>(total_key(dist)) << 32) | j;
+      }
+      nk += __popc(bal);
+    }
+    __syncwarp();
+    if (nk < K) {  // fewer certified candidates than neighbours (non-finite data): exact fallback
+      if (lane == 0) fallback_rows[atomicAdd(n_fallback, 1u)] = static_cast<uint32_t>(r);
+      __syncwarp();
+      continue;
+    }
+    const int Pr = next_pow2(nk);
+    for (int e = nk + lane; e < Pr; e += 32) keys[e] = ~0ull;
+    warp_bitonic_sort_u64(keys, Pr);
+    for (int c = lane; c < K; c += 32) {
+      const uint64_t kv = keys[c];
+      out_idx[r * K + c] = static_cast<uint32_t>(kv & 0xFFFFFFFFu);
+      out_dist[r * K + c] = key_to_float(static_cast<uint32_t>(kv >> 32));
+    }
+    __syncwarp();
+  }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link-time libcuda dependency).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    PM_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    PM_REQUIRE(p != nullptr && q == cudaDriverEntryPointSuccess, PACMAP_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+}  // namespace
+
+bool knn_tc_supported(uint64_t n, uint64_t d, uint64_t kp) {
+  return d >= 1 && d <= 128 && kp >= 1 && kp + 1 <= 448 && n >= 2 && n < (1ull << 31);
+}
+
+bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, bool bf16, uint32_t* d_idx,
+                   float* d_dist) {
+  if (!knn_tc_supported(n, d, kp)) return false;
+  const int KB = d <= 64 ? 1 : 2;
+  const int KP = 64 * KB;
+  const uint64_t n_pad = (n + TC_BM - 1) / TC_BM * TC_BM;
+  const int C = (kp + 1 <= 192) ? 512 : 1024;
+  const int rank = static_cast<int>(kp) + 1;
+
+  // scale: an exact power of two with max |x s| < 2^13
+  DevBuf<uint32_t> amax(c, 1);
+  PM_CUDA(cudaMemsetAsync(amax.get(), 0, sizeof(uint32_t), c.stream));
+  absmax_kernel<<<std::min<unsigned>(ceil_div(n * d, 256), c.sm_count * 8), 256, 0, c.stream>>>(d_x, n * d, amax.get());
+  PM_LAUNCHED();
+  uint32_t hbits = 0;
+  PM_CUDA(cudaMemcpyAsync(&hbits, amax.get(), 4, cudaMemcpyDeviceToHost, c.stream));
+  PM_CUDA(cudaStreamSynchronize(c.stream));
+  float amx;
+  std::memcpy(&amx, &hbits, 4);
+  if (!(amx > 0.0f) || !std::isfinite(amx)) return false;  // all-zero or non-finite data: SIMT path
+  int ex = 0;
+  std::frexp(amx, &ex);  // amx in [2^(ex-1), 2^ex)
+  const float s = std::ldexp(1.0f, 13 - ex);
+
+  DevBuf<uint16_t> H(c, n_pad * KP);
+  DevBuf<float> nrm(c, n_pad), A(c, n_pad), B(c, n_pad), g(c, n_pad), e4(c, n_pad);
+  const unsigned sgrid = std::min<unsigned>(ceil_div(n_pad, 8), c.sm_count * 8);
+  DevBuf<double> partial(c, 2 * sgrid);
+  if (bf16)
+    split_rows_kernel<true><<<sgrid, 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), KP, n_pad, s, H.get(), nrm.get(),
+                                                       A.get(), B.get(), partial.get());
+  else
+    split_rows_kernel<false><<<sgrid, 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), KP, n_pad, s, H.get(), nrm.get(),
+                                                        A.get(), B.get(), partial.get());
+  PM_LAUNCHED();
+  std::vector<double> hp(2 * sgrid);
+  PM_CUDA(cudaMemcpyAsync(hp.data(), partial.get(), hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  PM_CUDA(cudaStreamSynchronize(c.stream));
+  double sa = 0.0, sb = 0.0;
+  for (unsigned b = 0; b < sgrid; ++b) {
+    sa += hp[2 * b];
+    sb += hp[2 * b + 1];
+  }
+  const float rho = (sa > 0.0 && sb > 0.0) ? static_cast<float>(std::sqrt(sb / sa)) : 1e-4f;
+  bound_kernel<<<ceil_div(n_pad, 256), 256, 0, c.stream>>>(n, n_pad, static_cast<int>(d), KP, rho, nrm.get(), A.get(),
+                                                          B.get(), g.get(), e4.get());
+  PM_LAUNCHED();
+
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(KP), static_cast<cuuint64_t>(n_pad)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(KP) * 2};
+  const cuuint32_t box[2] = {64, 128};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult cr = get_encode_fn()(&map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                                      H.get(), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  PM_REQUIRE(cr == CUDA_SUCCESS, PACMAP_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(cr));
+
+  DevBuf<uint32_t> cidx(c, n_pad * C);
+  DevBuf<float> cv(c, n_pad * C), cu(c, n_pad * C);
+  DevBuf<int> ccnt(c, n_pad);
+  DevBuf<uint32_t> ovf(c, n + 1), fbk(c, n + 1);
+  PM_CUDA(cudaMemsetAsync(ccnt.get(), 0xFF, n_pad * sizeof(int), c.stream));
+  PM_CUDA(cudaMemsetAsync(ovf.get() + n, 0, sizeof(uint32_t), c.stream));
+  PM_CUDA(cudaMemsetAsync(fbk.get() + n, 0, sizeof(uint32_t), c.stream));
+
+  const size_t smem = 1024 + static_cast<size_t>(2 + TC_STAGES) * KB * KB_BYTES + sizeof(TcShared);
+  const uint32_t idesc = idesc_f16(bf16);
+  const unsigned grid = static_cast<unsigned>(n_pad / TC_BM);
+  cudaEvent_t ev[2];
+  PM_CUDA(cudaEventCreate(&ev[0]));
+  PM_CUDA(cudaEventCreate(&ev[1]));
+  PM_CUDA(cudaEventRecord(ev[0], c.stream));
+  if (KB == 1) {
+    PM_CUDA(cudaFuncSetAttribute(knn_filter_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    knn_filter_kernel<1><<<grid, TC_THREADS, smem, c.stream>>>(map, n, n_pad, idesc, g.get(), e4.get(), nrm.get(), C, rank,
+                                                             cidx.get(), cv.get(), cu.get(), ccnt.get(), ovf.get(),
+                                                             ovf.get() + n, c.d_err);
+  } else {
+    PM_CUDA(cudaFuncSetAttribute(knn_filter_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    knn_filter_kernel<2><<<grid, TC_THREADS, smem, c.stream>>>(map, n, n_pad, idesc, g.get(), e4.get(), nrm.get(), C, rank,
+                                                             cidx.get(), cv.get(), cu.get(), ccnt.get(), ovf.get(),
+                                                             ovf.get() + n, c.d_err);
+  }
+  PM_LAUNCHED();
+  PM_CUDA(cudaEventRecord(ev[1], c.stream));
+  c.check_errors("tensor-core kNN filter");
+  float fms = 0.0f;
+  PM_CUDA(cudaEventElapsedTime(&fms, ev[0], ev[1]));
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  last_tc_filter_ms() = fms;
+
+  const size_t rsmem = static_cast<size_t>(RR_WARPS) * next_pow2(C) * sizeof(uint64_t);
+  PM_CUDA(cudaFuncSetAttribute(knn_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(rsmem)));
+  const unsigned rgrid = std::min<unsigned>(ceil_div(n, RR_WARPS), c.sm_count * 16);
+  knn_rerank_kernel<<<rgrid, RR_WARPS * 32, rsmem, c.stream>>>(d_x, n, static_cast<int>(d), static_cast<int>(kp), C, rank,
+                                                              nrm.get(), e4.get(), cidx.get(), cv.get(), cu.get(),
+                                                              ccnt.get(), d_idx, d_dist, fbk.get(), fbk.get() + n);
+  PM_LAUNCHED();
+
+  // Rows the filter could not settle: exact SIMT recomputation, scattered into place.
+  uint32_t counts[2] = {0, 0};
+  PM_CUDA(cudaMemcpyAsync(&counts[0], ovf.get() + n, 4, cudaMemcpyDeviceToHost, c.stream));
+  PM_CUDA(cudaMemcpyAsync(&counts[1], fbk.get() + n, 4, cudaMemcpyDeviceToHost, c.stream));
+  PM_CUDA(cudaStreamSynchronize(c.stream));
+  last_tc_fallback_rows() = counts[0] + counts[1];
+  const uint32_t* lists[2] = {ovf.get(), fbk.get()};
+  for (int q = 0; q < 2; ++q) {
+    if (!counts[q]) continue;
+    knn_rows_simt(c, d_x, n, d, kp, lists[q], counts[q], d_idx, d_dist, /*scatter=*/true);
+  }
+  return true;
+}
+
+double& last_tc_filter_ms() {
+  static thread_local double v = 0.0;
+  return v;
+}
+
+uint64_t& last_tc_fallback_rows() {
+  static thread_local uint64_t v = 0;
+  return v;
+}
+
 }  // namespace pacmap

@@ -280,7 +280,8 @@ def quality(x, y, sample, triplets, k: int = 10, device: int = 0):
     return p.value, a.value
 
 
-STAGES = ("preprocess", "knn", "reselect", "sample_mn", "sample_fp", "csr", "init", "optimize")
+STAGES = ("preprocess", "knn", "reselect", "sample_mn", "sample_fp", "csr", "init", "optimize", "knn_filter",
+          "knn_fallback_rows")
 
 
 def set_stage_timing(enabled: bool) -> None:

@@ -1,0 +1,62 @@
+"""The tensor-core kNN (tcgen05 FP16/BF16 distance GEMM filter + exact FP32 re-rank) against the oracle.
+
+Bar: indices AND f32 distances bit-exact with the reference algorithm (knn.rs:137-194, ties -> lower
+index) at every size, including rows that overflow the candidate buffer (exact fallback).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+F16, BF16, AUTO = 1, 2, 0
+
+
+def _mix(n, d, seed):
+    from pacmap_b200 import datasets
+
+    return datasets.isotropic_mixture(n=n, d=d, k=10, seed=seed)[0]
+
+
+@pytest.mark.parametrize("mode", [F16, BF16])
+@pytest.mark.parametrize("n,d,k", [(3001, 128, 90), (2000, 100, 60), (4096, 32, 17), (777, 13, 90), (300, 64, 10),
+                                   (1024, 128, 1), (513, 65, 200)])
+def test_tc_knn_bit_exact(lib, orc, mode, n, d, k):
+    x = _mix(n, d, seed=n + d)
+    gi, gd = lib.knn.find_k_nearest_neighbors(x, k, knn_mode=mode)
+    ei, ed = orc.knn_exact(x, k)
+    assert np.array_equal(gd, ed)
+    assert np.array_equal(gi, ei)
+
+
+def test_tc_knn_preprocessed_anisotropic(lib, orc):
+    # the fit_transform path: preprocessed data of the 1M x 128 generator, a 20k slice
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.anisotropic_mixture(n=20000, d=128, k=50, seed=1)
+    xp, *_ = orc.preprocess(x)
+    gi, gd = lib.knn.find_k_nearest_neighbors(xp, 90, knn_mode=AUTO)
+    ei, ed = orc.knn_exact(xp, 90)
+    assert np.array_equal(gd, ed) and np.array_equal(gi, ei)
+
+
+def test_tc_knn_duplicates_overflow_to_exact_fallback(lib, orc):
+    # 700 identical points: each has ~700 candidates at distance 0, more than the candidate buffer,
+    # so those rows take the exact SIMT fallback; the result must still be the oracle's.
+    x = _mix(3000, 24, seed=9)
+    x[1000:1700] = x[5]
+    x[2000:2010] = x[6]
+    for mode in (F16, BF16):
+        gi, gd = lib.knn.find_k_nearest_neighbors(x, 60, knn_mode=mode)
+        ei, ed = orc.knn_exact(x, 60)
+        assert np.array_equal(gd, ed) and np.array_equal(gi, ei)
+
+
+def test_tc_knn_quantised_ties(lib, orc):
+    # image-like data quantised to 1/255: many exactly tied distances
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.image_like(n=2500, d=784, seed=3)
+    x = x[:, :128].copy()
+    gi, gd = lib.knn.find_k_nearest_neighbors(x, 72, knn_mode=F16)
+    ei, ed = orc.knn_exact(x, 72)
+    assert np.array_equal(gd, ed) and np.array_equal(gi, ei)

@@ -178,10 +178,20 @@ def test_each_iteration_matches_oracle(lib, orc, itr):
     gg = lib.stages.optimize_steps(yg, mg, vg, pnn, pmn, pfp, 1.0, 100, 100, itr, itr + 1)
     yo, mo, vo = y0.copy(), m0.copy(), v0.copy()
     go, g64, absum = orc.step(yo, mo, vo, pnn, pmn, pfp, 1.0, 100, 100, itr)
+    # (1) the gradient: within 1e-5 of the row's sum of |contributions| (any summation order is the
+    #     reference's; gradient.rs:53-70 reduces in an unspecified order)
     assert (np.abs(gg[:-1] - go[:-1]) <= GRAD_TOL * absum + 1e-30).all()
-    assert np.abs(yg - yo).max() <= EMB_TOL * np.abs(yo).max()
+    # (2) Adam (adam.rs:35-60) applied to the GPU's own gradient reproduces y, m, v bit for bit
+    ya, ma, va = y0.copy(), m0.copy(), v0.copy()
+    orc.adam(ya, gg, ma, va, 1.0, itr)
+    assert np.array_equal(yg, ya) and np.array_equal(mg, ma) and np.array_equal(vg, va)
+    # (3) the embedding against the oracle's: 1e-5 normwise. At itr 0 (m = v = 0) Adam's step is close
+    #     to sign(g) * lr_t and amplifies the order-dependent rounding of near-zero gradients, so the
+    #     bound there is the propagated one (checked via (1) + (2)) and 1e-4 normwise.
+    tol = EMB_TOL if itr > 0 else 10 * EMB_TOL
+    assert np.abs(yg - yo).max() <= tol * np.abs(yo).max()
     assert np.abs(mg - mo).max() <= EMB_TOL * max(np.abs(mo).max(), 1e-30)
-    assert np.abs(vg - vo).max() <= EMB_TOL * max(np.abs(vo).max(), 1e-30)
+    assert np.abs(vg - vo).max() <= tol * max(np.abs(vo).max(), 1e-30)
 
 
 def test_trajectory_tracks_oracle(lib, orc):
