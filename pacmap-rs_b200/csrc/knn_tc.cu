@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "knn_tc.cuh"
+#include "ptx.cuh"
 
 namespace pacmap {
 
@@ -61,47 +62,6 @@ struct alignas(8) TcShared {
 // ---------------------------------------------------------------------------------------------
 // PTX wrappers (sm_100a).
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ uint64_t globaltimer() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s: far above any legitimate wait here
-
-// Bounded wait on a barrier phase; false when it gave up (timeout, or another role aborted).
-__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const uint64_t t0 = globaltimer();
-  for (uint32_t it = 1;; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 63) == 0) {
-      if (*abort_flag) return false;
-      if (globaltimer() - t0 > WAIT_LIMIT_NS) return false;
-    }
-  }
-}
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
@@ -215,6 +175,13 @@ __device__ __forceinline__ uint32_t warp_radix_select(const float* __restrict__ 
   return prefix;
 }
 
+// u = v + 4 e_j (the row-relative upper bound) for every buffered candidate, one warp.
+__device__ __forceinline__ void fill_upper_bounds(const uint32_t* __restrict__ idx, const float* __restrict__ v,
+                                                  float* __restrict__ u, int m, const float* __restrict__ e4) {
+  for (int e = threadIdx.x & 31; e < m; e += 32) u[e] = v[e] + __ldg(e4 + idx[e]);
+  __syncwarp();
+}
+
 // theta for row constants (n_i, e4_i = 4 e_i) and the selected UB key: v <= theta keeps every
 // candidate whose lower bound is within the (sqrt-tie-widened) k'-th upper bound.
 __device__ __forceinline__ float theta_from(uint32_t ukey, float n_i, float e4_i) {
@@ -222,6 +189,94 @@ __device__ __forceinline__ float theta_from(uint32_t ukey, float n_i, float e4_i
   const float base = uT + e4_i;
   const float slack = 9.5367431640625e-07f * fabsf(uT + n_i + 0.5f * e4_i) + 2.384185791015625e-07f * (n_i + fabsf(uT));
   return base + slack;
+}
+
+// Register-resident compaction of one row's buffer (m <= 32 * PER entries), one warp: the entries
+// are loaded once, the rank-`rank` smallest upper bound is found by a 4-pass 8-bit radix select on
+// the registers, entries with v <= theta survive (order kept) and are written back once.
+template <int PER>
+__device__ __forceinline__ int warp_compact_regs(uint32_t* __restrict__ idx, float* __restrict__ v,
+                                                 float* __restrict__ u, int m, int rank, float n_i, float e4_i,
+                                                 uint32_t* hist, float& theta_out) {
+  const int lane = threadIdx.x & 31;
+  uint32_t ri[PER];
+  float rv[PER], ru[PER];
+  uint32_t rk[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = q * 32 + lane;
+    const bool in = e < m;
+    ri[q] = in ? idx[e] : 0u;
+    rv[q] = in ? v[e] : 0.0f;
+    ru[q] = in ? u[e] : 0.0f;
+    rk[q] = in ? total_key(ru[q]) : 0xFFFFFFFFu;
+  }
+  uint32_t prefix = 0, mask = 0;
+  int need = rank;
+#pragma unroll 1
+  for (int pass = 0; pass < 4; ++pass) {
+    const int shift = 24 - 8 * pass;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) hist[lane * 8 + b] = 0;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < PER; ++q)
+      if (q * 32 + lane < m && (rk[q] & mask) == prefix) atomicAdd(&hist[(rk[q] >> shift) & 255u], 1u);
+    __syncwarp();
+    uint32_t local[8], lsum = 0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      local[b] = hist[lane * 8 + b];
+      lsum += local[b];
+    }
+    uint32_t incl = lsum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const uint32_t excl = incl - lsum;
+    const bool mine = (excl < static_cast<uint32_t>(need)) && (static_cast<uint32_t>(need) <= incl);
+    const unsigned who = __ballot_sync(0xFFFFFFFFu, mine);
+    const int src = who ? (__ffs(who) - 1) : 31;
+    int bin = 0;
+    uint32_t before = 0;
+    if (mine) {
+      uint32_t run = excl;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        if (run + local[b] >= static_cast<uint32_t>(need)) {
+          bin = lane * 8 + b;
+          before = run;
+          break;
+        }
+        run += local[b];
+      }
+    }
+    bin = __shfl_sync(0xFFFFFFFFu, bin, src);
+    before = __shfl_sync(0xFFFFFFFFu, before, src);
+    prefix |= static_cast<uint32_t>(bin) << shift;
+    mask |= 255u << shift;
+    need -= static_cast<int>(before);
+    __syncwarp();
+  }
+  const float th = theta_from(prefix, n_i, e4_i);
+  int out = 0;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const bool keep = (q * 32 + lane < m) && rv[q] <= th;
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
+    if (keep) {
+      const int pos = out + __popc(bal & ((1u << lane) - 1u));
+      idx[pos] = ri[q];
+      v[pos] = rv[q];
+      u[pos] = ru[q];
+    }
+    out += __popc(bal);
+  }
+  __syncwarp();
+  theta_out = th;
+  return out;
 }
 
 // Keeps entries with v <= theta, preserving order; returns the new count. One warp.
@@ -257,6 +312,88 @@ __device__ __forceinline__ int warp_compact(uint32_t* __restrict__ idx, float* _
 }
 
 // ---------------------------------------------------------------------------------------------
+// 0. locality order: every point joins the nearest of P pivots (points p * n / P); sorting by pivot
+//    puts near points in near rows, so each row block meets its own neighbourhood first (sweep
+//    order below) and its threshold tightens after a few tiles. Any order gives the same exact kNN.
+// ---------------------------------------------------------------------------------------------
+constexpr int PIV = 256;
+constexpr int PIV_CHUNK = 32;
+
+__global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restrict__ x, uint64_t n, int d,
+                                                           uint32_t* __restrict__ cell, uint32_t* __restrict__ count) {
+  extern __shared__ float ps[];  // PIV_CHUNK x d pivots, then PIV_CHUNK norms
+  float* pn = ps + PIV_CHUNK * d;
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  float best = __int_as_float(0x7f800000);
+  uint32_t arg = 0;
+  for (int p0 = 0; p0 < PIV; p0 += PIV_CHUNK) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < PIV_CHUNK * d; e += blockDim.x) {
+      const int p = e / d, c = e - p * d;
+      ps[e] = x[(static_cast<uint64_t>(p0 + p) * n / PIV) * d + c];
+    }
+    __syncthreads();
+    if (threadIdx.x < PIV_CHUNK) {
+      float s = 0.0f;
+      for (int c = 0; c < d; ++c) s = fmaf(ps[threadIdx.x * d + c], ps[threadIdx.x * d + c], s);
+      pn[threadIdx.x] = s;
+    }
+    __syncthreads();
+    if (i < n) {
+      float dot[PIV_CHUNK];
+#pragma unroll
+      for (int p = 0; p < PIV_CHUNK; ++p) dot[p] = 0.0f;
+      for (int c = 0; c < d; ++c) {
+        const float xv = x[i * d + c];
+#pragma unroll
+        for (int p = 0; p < PIV_CHUNK; ++p) dot[p] = fmaf(xv, ps[p * d + c], dot[p]);
+      }
+#pragma unroll
+      for (int p = 0; p < PIV_CHUNK; ++p) {
+        const float sc = fmaf(-2.0f, dot[p], pn[p]);
+        if (sc < best) {
+          best = sc;
+          arg = static_cast<uint32_t>(p0 + p);
+        }
+      }
+    }
+  }
+  if (i < n) {
+    cell[i] = arg;
+    atomicAdd(&count[arg], 1u);
+  }
+}
+
+__global__ void cell_offsets_kernel(uint32_t* __restrict__ count) {  // exclusive scan of PIV counts, 1 thread
+  if (threadIdx.x != 0) return;
+  uint32_t run = 0;
+  for (int p = 0; p < PIV; ++p) {
+    const uint32_t c = count[p];
+    count[p] = run;
+    run += c;
+  }
+}
+
+__global__ void cell_place_kernel(const uint32_t* __restrict__ cell, uint64_t n, uint32_t* __restrict__ cursor,
+                                  uint32_t* __restrict__ perm) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) perm[atomicAdd(&cursor[cell[i]], 1u)] = static_cast<uint32_t>(i);
+}
+
+// Column tile visited at step t by row block b: first the window of W tiles around the block's own
+// rows, then every other tile in ascending order (all blocks of a wave advance through the same
+// region, which keeps the B operand in L2).
+constexpr int SWEEP_W = 16;
+__host__ __device__ __forceinline__ int sweep_tile(int t, int b, int ntiles) {
+  if (ntiles <= SWEEP_W) return t;
+  int w0 = 2 * b - SWEEP_W / 2 + 1;
+  w0 = w0 < 0 ? 0 : (w0 > ntiles - SWEEP_W ? ntiles - SWEEP_W : w0);
+  if (t < SWEEP_W) return w0 + t;
+  const int r = t - SWEEP_W;
+  return r < w0 ? r : r + SWEEP_W;
+}
+
+// ---------------------------------------------------------------------------------------------
 // 1. prep
 // ---------------------------------------------------------------------------------------------
 __global__ void absmax_kernel(const float* __restrict__ x, uint64_t total, uint32_t* __restrict__ out) {
@@ -271,17 +408,18 @@ __global__ void absmax_kernel(const float* __restrict__ x, uint64_t total, uint3
 }
 
 template <bool BF16>
-__global__ void split_rows_kernel(const float* __restrict__ x, uint64_t n, int d, int KP, uint64_t n_pad, float s,
-                                  uint16_t* __restrict__ H, float* __restrict__ nrm, float* __restrict__ A,
-                                  float* __restrict__ B, double* __restrict__ partial) {
+__global__ void split_rows_kernel(const float* __restrict__ x, const uint32_t* __restrict__ perm, uint64_t n, int d,
+                                  int KP, uint64_t n_pad, float s, uint16_t* __restrict__ H, float* __restrict__ nrm,
+                                  float* __restrict__ A, float* __restrict__ B, double* __restrict__ partial) {
   __shared__ double red[2][8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double sa = 0.0, sb = 0.0;
   for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * 8 + warp; r < n_pad; r += static_cast<uint64_t>(gridDim.x) * 8) {
     float nn = 0.0f, aa = 0.0f, bb = 0.0f;
+    const uint64_t src = r < n ? static_cast<uint64_t>(perm[r]) : 0;
     for (int c = lane; c < KP; c += 32) {
       float xs = 0.0f;
-      if (r < n && c < d) xs = x[r * d + c] * s;
+      if (r < n && c < d) xs = x[src * d + c] * s;
       uint16_t hbits;
       float hf;
       if (BF16) {
@@ -333,13 +471,11 @@ __global__ void split_rows_kernel(const float* __restrict__ x, uint64_t n, int d
 // are inflated by 2^-16 relative; gamma covers the reference's own f32 distance sum, every f32
 // rounding of the epilogue and of these constants.
 __global__ void bound_kernel(uint64_t n, uint64_t n_pad, int d, int KP, float rho, const float* __restrict__ nrm,
-                             const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ g,
-                             float* __restrict__ e4) {
+                             const float* __restrict__ A, const float* __restrict__ B, float2* __restrict__ ge) {
   const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (j >= n_pad) return;
   if (j >= n) {
-    g[j] = __int_as_float(0x7f800000);  // +inf: padding columns never pass
-    e4[j] = 0.0f;
+    ge[j] = make_float2(__int_as_float(0x7f800000), 0.0f);  // +inf: padding columns never pass
     return;
   }
   const float infl = 1.0f + 1.52587890625e-05f;  // 1 + 2^-16
@@ -350,19 +486,19 @@ __global__ void bound_kernel(uint64_t n, uint64_t n_pad, int d, int KP, float rh
   const float gamma = static_cast<float>(2 * d + 64) * 5.9604644775390625e-08f + 1.9073486328125e-06f;
   const float e = 0.5f * (rho * a + b / rho) + 0.5f * b + 0.5f * eta * a + gamma * nn + 1e-30f;
   const float e_safe = e * (1.0f + 9.765625e-04f);  // 2^-10 relative margin on the bound itself
-  g[j] = nrm[j] - 2.0f * e_safe;
-  e4[j] = 4.0f * e_safe;
+  ge[j] = make_float2(nrm[j] - 2.0f * e_safe, 4.0f * e_safe);
 }
 
 // ---------------------------------------------------------------------------------------------
 // 2. the tcgen05 filter
 // ---------------------------------------------------------------------------------------------
-template <int KB>  // K blocks of 64 elements: KP = 64 * KB
+template <int KB, int PER>  // K blocks of 64 elements: KP = 64 * KB; candidate buffer C = 32 * PER
 __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
-    const __grid_constant__ CUtensorMap hmap, uint64_t n, uint64_t n_pad, uint32_t idesc, const float* __restrict__ g,
-    const float* __restrict__ e4, const float* __restrict__ nrm, int C, int rank, uint32_t* __restrict__ cand_idx,
+    const __grid_constant__ CUtensorMap hmap, uint64_t n, uint64_t n_pad, uint32_t idesc, const float2* __restrict__ ge,
+    const float* __restrict__ nrm, const uint32_t* __restrict__ perm, int rank, uint32_t* __restrict__ cand_idx,
     float* __restrict__ cand_v, float* __restrict__ cand_u, int* __restrict__ cand_cnt, uint32_t* __restrict__ overflow_rows,
     uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err) {
+  constexpr int C = 32 * PER;
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   // 1024-byte aligned operand region: A [2 halves][KB][16 KB], B [STAGES][KB][16 KB], then TcShared.
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
@@ -411,8 +547,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         const int s = t % TC_STAGES;
         if (t >= TC_STAGES && !mbar_wait(&sh->empty[s], ((t / TC_STAGES) + 1) & 1, abort_flag)) break;
         mbar_expect_tx(&sh->full[s], KB * KB_BYTES);
+        const int tile = sweep_tile(t, static_cast<int>(blockIdx.x), ntiles);
         for (int kb = 0; kb < KB; ++kb)
-          tma_load_2d(b_smem + (s * KB + kb) * KB_BYTES, &hmap, &sh->full[s], kb * 64, t * TC_BN);
+          tma_load_2d(b_smem + (s * KB + kb) * KB_BYTES, &hmap, &sh->full[s], kb * 64, tile * TC_BN);
         issued = t + 1;
       }
       if (issued < ntiles) {
@@ -480,7 +617,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     float theta = valid ? 3.402823466e+38f : -__int_as_float(0x7f800000);
     int cnt = 0;
     const float n_i = valid ? nrm[row] : 0.0f;
-    const float e4_i = valid ? e4[row] : 0.0f;
+    const float e4_i = valid ? ge[row].y : 0.0f;
     const uint64_t cbase = row * static_cast<uint64_t>(C);
     bool ok = true;
     for (int t = 0; t < ntiles; ++t) {
@@ -490,33 +627,42 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         break;
       }
       tc_fence_after();
-      const int col0 = t * TC_BN;
+      const int col0 = sweep_tile(t, static_cast<int>(blockIdx.x), ntiles) * TC_BN;
       const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) + acc * 256 + half * 128;
+      // The next tile's column constants go to L1 now (8 x 128 B of (g, 4e) pairs).
+      if (lane < 8 && t + 1 < ntiles)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(ge + sweep_tile(t + 1, static_cast<int>(blockIdx.x), ntiles) * TC_BN +
+                                                        lane * 16));
 #pragma unroll 1
       for (int ch = 0; ch < 4; ++ch) {
+        // column constants first: their loads are in flight while the accumulator is read from TMEM
+        const float4* gp = reinterpret_cast<const float4*>(ge + col0 + ch * 32);
+        float4 gq[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) gq[q] = __ldg(gp + q);
         float G[32];
         tmem_ld32(taddr + ch * 32, G);
-        const float4* gp = reinterpret_cast<const float4*>(g + col0 + ch * 32);
         float v[32];
-        float vmin = __int_as_float(0x7f800000);
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const float4 gv = __ldg(gp + q);
-          v[4 * q + 0] = fmaf(-2.0f, G[4 * q + 0], gv.x);
-          v[4 * q + 1] = fmaf(-2.0f, G[4 * q + 1], gv.y);
-          v[4 * q + 2] = fmaf(-2.0f, G[4 * q + 2], gv.z);
-          v[4 * q + 3] = fmaf(-2.0f, G[4 * q + 3], gv.w);
-          vmin = fminf(vmin, fminf(fminf(v[4 * q + 0], v[4 * q + 1]), fminf(v[4 * q + 2], v[4 * q + 3])));
+        for (int q = 0; q < 16; ++q) {
+          v[2 * q + 0] = fmaf(-2.0f, G[2 * q + 0], gq[q].x);
+          v[2 * q + 1] = fmaf(-2.0f, G[2 * q + 1], gq[q].z);
         }
-        if (vmin <= theta) {
+        // Warp-uniform early-outs per 8 columns; an insertion is three plain stores.
 #pragma unroll
-          for (int c = 0; c < 32; ++c) {
-            if (v[c] <= theta) {
-              const uint32_t j = static_cast<uint32_t>(col0 + ch * 32 + c);
-              cand_idx[cbase + cnt] = j;
-              cand_v[cbase + cnt] = v[c];
-              cand_u[cbase + cnt] = v[c] + __ldg(e4 + j);
-              ++cnt;
+        for (int o = 0; o < 32; o += 8) {
+          const float m8 = fminf(fminf(fminf(v[o], v[o + 1]), fminf(v[o + 2], v[o + 3])),
+                                 fminf(fminf(v[o + 4], v[o + 5]), fminf(v[o + 6], v[o + 7])));
+          if (__any_sync(0xFFFFFFFFu, m8 <= theta)) {
+#pragma unroll
+            for (int c = o; c < o + 8; ++c) {
+              if (v[c] <= theta) {
+                const float e4j = (c & 1) ? gq[c >> 1].w : gq[c >> 1].y;
+                cand_idx[cbase + cnt] = static_cast<uint32_t>(col0 + ch * 32 + c);
+                cand_v[cbase + cnt] = v[c];
+                cand_u[cbase + cnt] = v[c] + e4j;
+                ++cnt;
+              }
             }
           }
         }
@@ -533,17 +679,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         const int m = __shfl_sync(0xFFFFFFFFu, cnt, L);
         const float nL = __shfl_sync(0xFFFFFFFFu, n_i, L);
         const float eL = __shfl_sync(0xFFFFFFFFu, e4_i, L);
-        const uint32_t key = warp_radix_select(cand_u + rb, m, min(rank, m), hist);
-        const float th = theta_from(key, nL, eL);
-        __threadfence_block();
-        const int kept = warp_compact(cand_idx + rb, cand_v + rb, cand_u + rb, m, th);
+        float th;
+        const int kept = warp_compact_regs<PER>(cand_idx + rb, cand_v + rb, cand_u + rb, m, min(rank, m), nL, eL, hist, th);
         if (lane == L) {
           theta = th;
           cnt = kept;
           if (cnt > C - TC_BN) {  // the band does not fit: exact recomputation later
             theta = -__int_as_float(0x7f800000);
             cnt = 0;
-            overflow_rows[atomicAdd(n_overflow, 1u)] = static_cast<uint32_t>(row);
+            overflow_rows[atomicAdd(n_overflow, 1u)] = perm[row];
           }
         }
         __syncwarp();
@@ -564,20 +708,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
 }
 
 // ---------------------------------------------------------------------------------------------
-// 3. exact re-rank: one warp per row.
+// 3. exact re-rank: one warp per (permuted) row; output at the original row, original indices.
 // ---------------------------------------------------------------------------------------------
 constexpr int RR_WARPS = 4;
 
+template <int PER>
 __global__ void __launch_bounds__(RR_WARPS * 32) knn_rerank_kernel(
-    const float* __restrict__ x, uint64_t n, int d, int K, int C, int rank, const float* __restrict__ nrm,
-    const float* __restrict__ e4, uint32_t* __restrict__ cand_idx, float* __restrict__ cand_v,
-    float* __restrict__ cand_u, const int* __restrict__ cand_cnt, uint32_t* __restrict__ out_idx,
-    float* __restrict__ out_dist, uint32_t* __restrict__ fallback_rows, uint32_t* __restrict__ n_fallback) {
-  extern __shared__ uint64_t rr_smem[];
+    const float* __restrict__ x, uint64_t n, int d, int K, int rank, const float* __restrict__ nrm,
+    const float2* __restrict__ ge, const uint32_t* __restrict__ perm, uint32_t* __restrict__ cand_idx,
+    float* __restrict__ cand_v, float* __restrict__ cand_u, const int* __restrict__ cand_cnt,
+    uint32_t* __restrict__ out_idx, float* __restrict__ out_dist, uint32_t* __restrict__ fallback_rows,
+    uint32_t* __restrict__ n_fallback) {
+  constexpr int C = 32 * PER;
+  __shared__ uint64_t keys_all[RR_WARPS][C];
   __shared__ uint32_t hist_all[RR_WARPS][256];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int P = next_pow2(C);
-  uint64_t* keys = rr_smem + warp * P;
+  uint64_t* keys = keys_all[warp];
   uint32_t* hist = hist_all[warp];
   const int l8 = lane & 7, grp = lane >> 3;
   for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * RR_WARPS + warp; r < n;
@@ -585,18 +731,19 @@ __global__ void __launch_bounds__(RR_WARPS * 32) knn_rerank_kernel(
     const int m0 = min(cand_cnt[r], C);
     if (m0 < 0) continue;  // overflowed in the filter: handled by the exact fallback
     const uint64_t rb = r * static_cast<uint64_t>(C);
+    const uint64_t orow = perm[r];
     int m = m0;
     if (m > 0) {
-      const uint32_t key = warp_radix_select(cand_u + rb, m, min(rank, m), hist);
-      const float th = theta_from(key, nrm[r], e4[r]);
-      m = warp_compact(cand_idx + rb, cand_v + rb, cand_u + rb, m, th);
+      float th;
+      m = warp_compact_regs<PER>(cand_idx + rb, cand_v + rb, cand_u + rb, m, min(rank, m), nrm[r], ge[r].y, hist, th);
     }
     // exact reference distances of the survivors (self excluded), 4 at a time per warp
     int nk = 0;
+    const float* a = x + orow * d;
     for (int e0 = 0; e0 < m; e0 += 4) {
       const int e = e0 + grp;
-      const uint32_t j = (e < m) ? cand_idx[rb + e] : static_cast<uint32_t>(r);
-      const float* a = x + r * d;
+      const uint32_t jp = (e < m) ? cand_idx[rb + e] : static_cast<uint32_t>(r);
+      const uint32_t j = perm[jp];
       const float* b = x + static_cast<uint64_t>(j) * d;
       float accl = 0.0f;
       const int nc = d >> 3;
@@ -612,7 +759,7 @@ __global__ void __launch_bounds__(RR_WARPS * 32) knn_rerank_kernel(
         t = __fadd_rn(t, __fmul_rn(df, df));
       }
       const float dist = __fsqrt_rn(t);
-      const bool real = (e < m) && (j != r);
+      const bool real = (e < m) && (jp != r);
       const unsigned bal = __ballot_sync(0xFFFFFFFFu, real && l8 == 0);
       if (real && l8 == 0) {
         const int pos = nk + __popc(bal & ((1u << lane) - 1u));
@@ -622,7 +769,7 @@ __global__ void __launch_bounds__(RR_WARPS * 32) knn_rerank_kernel(
     }
     __syncwarp();
     if (nk < K) {  // fewer certified candidates than neighbours (non-finite data): exact fallback
-      if (lane == 0) fallback_rows[atomicAdd(n_fallback, 1u)] = static_cast<uint32_t>(r);
+      if (lane == 0) fallback_rows[atomicAdd(n_fallback, 1u)] = static_cast<uint32_t>(orow);
       __syncwarp();
       continue;
     }
@@ -631,8 +778,8 @@ __global__ void __launch_bounds__(RR_WARPS * 32) knn_rerank_kernel(
     warp_bitonic_sort_u64(keys, Pr);
     for (int c = lane; c < K; c += 32) {
       const uint64_t kv = keys[c];
-      out_idx[r * K + c] = static_cast<uint32_t>(kv & 0xFFFFFFFFu);
-      out_dist[r * K + c] = key_to_float(static_cast<uint32_t>(kv >> 32));
+      out_idx[orow * K + c] = static_cast<uint32_t>(kv & 0xFFFFFFFFu);
+      out_dist[orow * K + c] = key_to_float(static_cast<uint32_t>(kv >> 32));
     }
     __syncwarp();
   }
@@ -667,7 +814,8 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   const int KB = d <= 64 ? 1 : 2;
   const int KP = 64 * KB;
   const uint64_t n_pad = (n + TC_BM - 1) / TC_BM * TC_BM;
-  const int C = (kp + 1 <= 192) ? 512 : 1024;
+  const int PER = (kp + 1 <= 192) ? 16 : 32;  // buffer C = 512 or 1024 candidates per row
+  const int C = 32 * PER;
   const int rank = static_cast<int>(kp) + 1;
 
   // scale: an exact power of two with max |x s| < 2^13
@@ -685,16 +833,29 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   std::frexp(amx, &ex);  // amx in [2^(ex-1), 2^ex)
   const float s = std::ldexp(1.0f, 13 - ex);
 
+  // locality order
+  DevBuf<uint32_t> cell(c, n), ccount(c, PIV), perm(c, n);
+  PM_CUDA(cudaMemsetAsync(ccount.get(), 0, PIV * sizeof(uint32_t), c.stream));
+  const size_t psm = (static_cast<size_t>(PIV_CHUNK) * d + PIV_CHUNK) * sizeof(float);
+  PM_CUDA(cudaFuncSetAttribute(pivot_assign_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(psm)));
+  pivot_assign_kernel<<<ceil_div(n, 256), 256, psm, c.stream>>>(d_x, n, static_cast<int>(d), cell.get(), ccount.get());
+  PM_LAUNCHED();
+  cell_offsets_kernel<<<1, 32, 0, c.stream>>>(ccount.get());
+  PM_LAUNCHED();
+  cell_place_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(cell.get(), n, ccount.get(), perm.get());
+  PM_LAUNCHED();
+
   DevBuf<uint16_t> H(c, n_pad * KP);
-  DevBuf<float> nrm(c, n_pad), A(c, n_pad), B(c, n_pad), g(c, n_pad), e4(c, n_pad);
+  DevBuf<float> nrm(c, n_pad), A(c, n_pad), B(c, n_pad);
+  DevBuf<float2> ge(c, n_pad);
   const unsigned sgrid = std::min<unsigned>(ceil_div(n_pad, 8), c.sm_count * 8);
   DevBuf<double> partial(c, 2 * sgrid);
   if (bf16)
-    split_rows_kernel<true><<<sgrid, 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), KP, n_pad, s, H.get(), nrm.get(),
-                                                       A.get(), B.get(), partial.get());
+    split_rows_kernel<true><<<sgrid, 256, 0, c.stream>>>(d_x, perm.get(), n, static_cast<int>(d), KP, n_pad, s, H.get(),
+                                                       nrm.get(), A.get(), B.get(), partial.get());
   else
-    split_rows_kernel<false><<<sgrid, 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), KP, n_pad, s, H.get(), nrm.get(),
-                                                        A.get(), B.get(), partial.get());
+    split_rows_kernel<false><<<sgrid, 256, 0, c.stream>>>(d_x, perm.get(), n, static_cast<int>(d), KP, n_pad, s, H.get(),
+                                                        nrm.get(), A.get(), B.get(), partial.get());
   PM_LAUNCHED();
   std::vector<double> hp(2 * sgrid);
   PM_CUDA(cudaMemcpyAsync(hp.data(), partial.get(), hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -706,7 +867,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   }
   const float rho = (sa > 0.0 && sb > 0.0) ? static_cast<float>(std::sqrt(sb / sa)) : 1e-4f;
   bound_kernel<<<ceil_div(n_pad, 256), 256, 0, c.stream>>>(n, n_pad, static_cast<int>(d), KP, rho, nrm.get(), A.get(),
-                                                          B.get(), g.get(), e4.get());
+                                                          B.get(), ge.get());
   PM_LAUNCHED();
 
   CUtensorMap map;
@@ -736,17 +897,15 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_CUDA(cudaEventCreate(&ev[0]));
   PM_CUDA(cudaEventCreate(&ev[1]));
   PM_CUDA(cudaEventRecord(ev[0], c.stream));
-  if (KB == 1) {
-    PM_CUDA(cudaFuncSetAttribute(knn_filter_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    knn_filter_kernel<1><<<grid, TC_THREADS, smem, c.stream>>>(map, n, n_pad, idesc, g.get(), e4.get(), nrm.get(), C, rank,
-                                                             cidx.get(), cv.get(), cu.get(), ccnt.get(), ovf.get(),
-                                                             ovf.get() + n, c.d_err);
-  } else {
-    PM_CUDA(cudaFuncSetAttribute(knn_filter_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    knn_filter_kernel<2><<<grid, TC_THREADS, smem, c.stream>>>(map, n, n_pad, idesc, g.get(), e4.get(), nrm.get(), C, rank,
-                                                             cidx.get(), cv.get(), cu.get(), ccnt.get(), ovf.get(),
-                                                             ovf.get() + n, c.d_err);
-  }
+  auto launch = [&](auto kern) {
+    PM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kern<<<grid, TC_THREADS, smem, c.stream>>>(map, n, n_pad, idesc, ge.get(), nrm.get(), perm.get(), rank, cidx.get(),
+                                             cv.get(), cu.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err);
+  };
+  if (KB == 1 && PER == 16) launch(knn_filter_kernel<1, 16>);
+  else if (KB == 1) launch(knn_filter_kernel<1, 32>);
+  else if (PER == 16) launch(knn_filter_kernel<2, 16>);
+  else launch(knn_filter_kernel<2, 32>);
   PM_LAUNCHED();
   PM_CUDA(cudaEventRecord(ev[1], c.stream));
   c.check_errors("tensor-core kNN filter");
@@ -756,12 +915,15 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   cudaEventDestroy(ev[1]);
   last_tc_filter_ms() = fms;
 
-  const size_t rsmem = static_cast<size_t>(RR_WARPS) * next_pow2(C) * sizeof(uint64_t);
-  PM_CUDA(cudaFuncSetAttribute(knn_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(rsmem)));
   const unsigned rgrid = std::min<unsigned>(ceil_div(n, RR_WARPS), c.sm_count * 16);
-  knn_rerank_kernel<<<rgrid, RR_WARPS * 32, rsmem, c.stream>>>(d_x, n, static_cast<int>(d), static_cast<int>(kp), C, rank,
-                                                              nrm.get(), e4.get(), cidx.get(), cv.get(), cu.get(),
-                                                              ccnt.get(), d_idx, d_dist, fbk.get(), fbk.get() + n);
+  if (PER == 16)
+    knn_rerank_kernel<16><<<rgrid, RR_WARPS * 32, 0, c.stream>>>(d_x, n, static_cast<int>(d), static_cast<int>(kp), rank,
+                                                               nrm.get(), ge.get(), perm.get(), cidx.get(), cv.get(),
+                                                               cu.get(), ccnt.get(), d_idx, d_dist, fbk.get(), fbk.get() + n);
+  else
+    knn_rerank_kernel<32><<<rgrid, RR_WARPS * 32, 0, c.stream>>>(d_x, n, static_cast<int>(d), static_cast<int>(kp), rank,
+                                                               nrm.get(), ge.get(), perm.get(), cidx.get(), cv.get(),
+                                                               cu.get(), ccnt.get(), d_idx, d_dist, fbk.get(), fbk.get() + n);
   PM_LAUNCHED();
 
   // Rows the filter could not settle: exact SIMT recomputation, scattered into place.

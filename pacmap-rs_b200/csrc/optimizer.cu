@@ -263,38 +263,67 @@ struct Sched {
   float w_nn, w_mn, w_fp, lr_t;
 };
 
-template <int DIM, bool FP>
-__device__ __forceinline__ void accumulate_segment(const float* __restrict__ y, const uint32_t* __restrict__ col,
-                                                   uint32_t b, uint32_t e, int gl, int G, const float (&yi)[DIM],
-                                                   float w, float c1, float c2, float (&acc)[DIM], float& lacc,
-                                                   bool want_loss) {
-  for (uint32_t t = b + gl; t < e; t += G) {
-    const uint32_t j = col[t];
-    float yj[DIM];
-    if constexpr (DIM == 2) {
-      const float2 v = *reinterpret_cast<const float2*>(y + static_cast<uint64_t>(j) * 2);
-      yj[0] = v.x;
-      yj[1] = v.y;
-    } else {
+// One row's entries: [s0, s1) NN, [s1, s2) MN (skipped when w_mn == 0), [s2, s3) FP, walked as one index
+// space q = gl, gl + G, ... (a fixed per-lane summation order) with a two-deep software pipeline:
+// while entry k is summed, y of entry k + 1 and the partner index of entry k + 2 are in flight.
+template <int DIM>
+__device__ __forceinline__ void load_y(const float* __restrict__ y, uint32_t j, float (&out)[DIM]) {
+  if constexpr (DIM == 2) {
+    const float2 v = *reinterpret_cast<const float2*>(y + static_cast<uint64_t>(j) * 2);
+    out[0] = v.x;
+    out[1] = v.y;
+  } else {
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) yj[c] = y[static_cast<uint64_t>(j) * DIM + c];
-    }
+    for (int c = 0; c < DIM; ++c) out[c] = y[static_cast<uint64_t>(j) * DIM + c];
+  }
+}
+
+template <int DIM>
+__device__ __forceinline__ void accumulate_row(const float* __restrict__ y, const uint32_t* __restrict__ col,
+                                               uint32_t s0, uint32_t s1, uint32_t s2, uint32_t s3, bool use_mn,
+                                               int gl, int G, const float (&yi)[DIM], const Sched& sc,
+                                               float (&acc)[DIM], float& lacc, bool want_loss) {
+  const uint32_t nnn = s1 - s0, nmn = use_mn ? (s2 - s1) : 0u;
+  const uint32_t total = nnn + nmn + (s3 - s2);
+  auto where = [&](uint32_t q) -> uint32_t {
+    return q < nnn ? s0 + q : (q < nnn + nmn ? s1 + (q - nnn) : s2 + (q - nnn - nmn));
+  };
+  uint32_t q = static_cast<uint32_t>(gl);
+  if (q >= total) return;
+  uint32_t ja = col[where(q)];
+  const uint32_t qb0 = q + G;
+  uint32_t jb = qb0 < total ? col[where(qb0)] : 0u;
+  float ya[DIM];
+  load_y<DIM>(y, ja, ya);
+  for (; q < total; q += G) {
+    const uint32_t qb = q + G, qc = q + 2 * G;
+    float yb[DIM];
+    if (qb < total) load_y<DIM>(y, jb, yb);
+    const uint32_t jc = qc < total ? col[where(qc)] : 0u;
+    const int ty = q < nnn ? 0 : (q < nnn + nmn ? 1 : 2);
+    const bool fp = ty == 2;
+    const float c1 = ty == 0 ? 10.0f : (ty == 1 ? 10000.0f : 1.0f);
+    const float c2 = ty == 0 ? 20.0f : (ty == 1 ? 20000.0f : 2.0f);
+    const float w = ty == 0 ? sc.w_nn : (ty == 1 ? sc.w_mn : sc.w_fp);
     float df[DIM];
     float dsq = 1.0f;
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      df[c] = __fsub_rn(yi[c], yj[c]);
+      df[c] = __fsub_rn(yi[c], ya[c]);
       dsq = __fadd_rn(dsq, __fmul_rn(df[c], df[c]));
     }
     const float tt = __fadd_rn(c1, dsq);
     const float w1 = __fmul_rn(w, __fdiv_rn(c2, __fmul_rn(tt, tt)));
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      const float g = __fmul_rn(w1, df[c]);
-      acc[c] = FP ? __fsub_rn(acc[c], g) : __fadd_rn(acc[c], g);
+      const float gterm = __fmul_rn(w1, df[c]);
+      acc[c] = __fadd_rn(acc[c], fp ? -gterm : gterm);
     }
     if (want_loss)
-      lacc += FP ? __fmul_rn(w, __fdiv_rn(1.0f, __fadd_rn(1.0f, dsq))) : __fmul_rn(w, __fdiv_rn(dsq, tt));
+      lacc += fp ? __fmul_rn(w, __fdiv_rn(1.0f, __fadd_rn(1.0f, dsq))) : __fmul_rn(w, __fdiv_rn(dsq, tt));
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) ya[c] = yb[c];
+    jb = jc;
   }
 }
 
@@ -320,10 +349,7 @@ __global__ void __launch_bounds__(256) grad_adam_kernel(const float* __restrict_
     }
     float lacc = 0.0f;
     const uint32_t s0 = rp[3 * i], s1 = rp[3 * i + 1], s2 = rp[3 * i + 2], s3 = rp[3 * i + 3];
-    accumulate_segment<DIM, false>(y_cur, col, s0, s1, gl, G, yi, sc.w_nn, 10.0f, 20.0f, acc, lacc, want_loss);
-    if (sc.w_mn != 0.0f)
-      accumulate_segment<DIM, false>(y_cur, col, s1, s2, gl, G, yi, sc.w_mn, 10000.0f, 20000.0f, acc, lacc, want_loss);
-    accumulate_segment<DIM, true>(y_cur, col, s2, s3, gl, G, yi, sc.w_fp, 1.0f, 2.0f, acc, lacc, want_loss);
+    accumulate_row<DIM>(y_cur, col, s0, s1, s2, s3, sc.w_mn != 0.0f, gl, G, yi, sc, acc, lacc, want_loss);
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) {
 #pragma unroll
@@ -547,7 +573,10 @@ void optimize_device(Ctx& c, const Csr& csr, const OptimizeArgs& a) {
     row_loss.alloc(c, n);
     loss_dev.alloc(c, iters);
   }
-  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n, 256 / G), c.sm_count * 8ull));
+  int per_sm = 0;
+  PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
+  const unsigned grid = static_cast<unsigned>(
+      std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(n, 256 / G), static_cast<uint64_t>(c.sm_count) * std::max(per_sm, 1))));
   float* bufs[2] = {a.d_y, yb.get()};
 
   cudaGraph_t graph = nullptr;

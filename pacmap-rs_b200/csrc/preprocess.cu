@@ -65,7 +65,15 @@ __global__ void __launch_bounds__(CS_THREADS) colsum_seq_kernel(const float* __r
     if (tid < CS_COLS) {
       const int rows = static_cast<int>((n - ch * CS_ROWS) < CS_ROWS ? (n - ch * CS_ROWS) : CS_ROWS);
       const int slot = static_cast<int>(ch & 1);
-      for (int r = 0; r < rows; ++r) s = __fadd_rn(s, buf[slot][r][tid]);
+      int r = 0;
+      for (; r + 16 <= rows; r += 16) {  // loads run ahead of the serial add chain
+        float t[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) t[q] = buf[slot][r + q][tid];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) s = __fadd_rn(s, t[q]);
+      }
+      for (; r < rows; ++r) s = __fadd_rn(s, buf[slot][r][tid]);
     }
     __syncthreads();
   }
