@@ -186,6 +186,17 @@ pacmap_status pacmap_quality(const float* x, uint64_t n, uint64_t d, const float
                              uint64_t n_triplets, int32_t device, double* out_preservation,
                              double* out_triplet_accuracy);
 
+/* preprocess_x (the arithmetic of pacmap_preprocess) for callers that cannot allocate device memory --
+ * a process whose device memory belongs to another framework's allocator or to a fixed budget, or a
+ * latency-critical loop that must not reach cudaMalloc/cudaFree. No counterpart in the reference.
+ * d_x, d_out: n x d device buffers on `device`; `stream` is a cudaStream_t (NULL = legacy default
+ * stream). Stream-ordered: the call returns once the work is enqueued. The scratch is a fixed device
+ * array of the library (at most 16,384 columns; larger d returns PACMAP_ERR_UNSUPPORTED), looked up on
+ * the first call per device -- make that call before any stream capture. All calls share that array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+pacmap_status pacmap_preprocess_noalloc(const float* d_x, uint64_t n, uint64_t d, float* d_out, void* stream,
+                                        int32_t device);
+
 /* Stage timing (diagnostics): when enabled, each fit_transform records the device time of its stages
  * with CUDA events on its stream. pacmap_stage_times fills up to `cap` values in milliseconds, in the
  * order preprocess, knn, reselect, sample_mn, sample_fp, csr, init, optimize (then, when the tensor-core
