@@ -178,6 +178,35 @@ pacmap_status pacmap_init_value(const float* v, uint64_t n, uint64_t dim, int32_
 /* Initialization::Random(seed) on the library's Philox stream (N(0,1), Box-Muller). */
 pacmap_status pacmap_init_random(uint64_t n, uint64_t dim, uint64_t seed, int32_t device, float* out);
 
+/* --- the learned initialiser (no reference analogue) ---
+ * An MLP d -> 512 -> 512 -> dim (ReLU; BF16 weights and activations, FP32 accumulation; every GEMM a
+ * tcgen05 kernel) maps preprocessed data x' (the output of pacmap_preprocess) to an embedding, used as
+ * Initialization::Value (src/lib.rs:753-766) so that a shortened schedule suffices. Parameters are one
+ * flat f32 array: [W1 (512 x d), b1 (512), W2 (512 x 512), b2 (512), W3 (dim x 512), b3 (dim)]. */
+uint64_t pacmap_mlp_param_count(uint64_t d, uint64_t dim);
+/* Seeded U(-1/sqrt(fan_in), 1/sqrt(fan_in)) initial parameters. */
+pacmap_status pacmap_mlp_init(uint64_t d, uint64_t dim, uint64_t seed, float* out_params);
+/* AdamW training on (x' rows, target embedding rows; targets are z-scored per dimension), mean squared
+ * error, `epochs` passes in shuffled batches of `batch` rows (a multiple of 128). inout_params: the
+ * starting parameters, replaced by the trained ones. out_epoch_loss (optional): epochs values. */
+pacmap_status pacmap_mlp_train(const float* xp, const float* target, uint64_t n, uint64_t d, uint64_t dim,
+                               uint64_t epochs, uint64_t batch, float lr, float weight_decay, uint64_t seed,
+                               int32_t device, float* inout_params, float* out_epoch_loss);
+/* out (n x dim) = MLP(xp). */
+pacmap_status pacmap_mlp_apply(const float* params, uint64_t d, uint64_t dim, const float* xp, uint64_t n,
+                               int32_t device, float* out);
+/* Gradient of the mean squared error of one batch (batch a multiple of 128): out_grads in the flat
+ * parameter layout, out_loss the loss (the check against a CPU oracle). */
+pacmap_status pacmap_mlp_grad(const float* params, uint64_t d, uint64_t dim, const float* xp, const float* target,
+                              uint64_t batch, int32_t device, float* out_grads, float* out_loss);
+/* fit_transform (src/lib.rs:294-367) with the learned initialiser: the embedding starts from MLP(x')
+ * through Initialization::Value; cfg->init_kind is ignored. Use a shortened cfg->num_iters. */
+pacmap_status pacmap_fit_transform_learned(const float* x, uint64_t n, uint64_t d, const pacmap_config* cfg,
+                                           const float* mlp_params, float* out_embedding, float* out_snapshots);
+pacmap_status pacmap_fit_transform_learned_device(const float* d_x, uint64_t n, uint64_t d, const pacmap_config* cfg,
+                                                  const float* mlp_params, float* d_out_embedding,
+                                                  float* d_out_snapshots);
+
 /* Quality of an embedding (no reference analogue): mean 10-NN preservation over `sample` (n_sample
  * point indices; neighbours by the reference's f32 distance on the preprocessed data) and random-triplet
  * order accuracy over `triplets` (n_triplets x 3). x: raw n x d data; y: n x dim embedding. */

@@ -10,6 +10,7 @@
 
 #include "engine.cuh"
 #include "knn_tc.cuh"
+#include "mlp.cuh"
 
 namespace pacmap {
 
@@ -222,11 +223,11 @@ void validate_config(const pacmap_config* cfg) {
 
 // fit_transform with x already on the device; h_* pointers are the caller's host views of the config.
 void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const pacmap_config& cfg, float* d_out,
-                        float* d_snap) {
+                        float* d_snap, const float* mlp_params = nullptr) {
   // lib.rs:300-302
   PM_REQUIRE(n > 1, PACMAP_ERR_SAMPLE_SIZE, "Sample size must be larger than one");
   const uint64_t dim = cfg.embedding_dimensions;
-  PM_REQUIRE(cfg.init_kind != PACMAP_INIT_PCA, PACMAP_ERR_UNSUPPORTED,
+  PM_REQUIRE(cfg.init_kind != PACMAP_INIT_PCA || mlp_params != nullptr, PACMAP_ERR_UNSUPPORTED,
              "Initialization::Pca is not built in this engine; use Value or Random");
   PM_REQUIRE(dim <= 8, PACMAP_ERR_UNSUPPORTED, "embedding dimensions above 8 are not supported");
   StageTimer tm(c.stream);
@@ -272,7 +273,12 @@ void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const 
   if (dim == 0) return;
   // lib.rs:752-779 initial embedding
   tm.start(ST_INIT);
-  if (cfg.init_kind == PACMAP_INIT_VALUE) {
+  if (mlp_params) {
+    // learned initialiser: MLP(x') as Initialization::Value (lib.rs:753-766 z-scores it to std 1e-4)
+    DevBuf<float> raw(c, n * dim);
+    mlp_apply_device(c, mlp_params, d, dim, xp.get(), n, raw.get());
+    init_value_device(c, raw.get(), n, dim, d_out);
+  } else if (cfg.init_kind == PACMAP_INIT_VALUE) {
     PM_REQUIRE(cfg.init_value != nullptr, PACMAP_ERR_INVALID_ARGUMENT, "init_value is NULL");
     DevBuf<float> v;
     upload(c, v, cfg.init_value, n * dim);
@@ -388,6 +394,101 @@ pacmap_status pacmap_fit_transform_device(const float* d_x, uint64_t n, uint64_t
     DeviceLock dl(cfg->device);
     fit_transform_impl(dl.ctx, d_x, n, d, *cfg, d_out_embedding, d_out_snapshots);
     PM_CUDA(cudaStreamSynchronize(dl.ctx.stream));
+  });
+}
+
+pacmap_status pacmap_fit_transform_learned(const float* x, uint64_t n, uint64_t d, const pacmap_config* cfg,
+                                           const float* mlp_params, float* out_embedding, float* out_snapshots) {
+  return guarded([&] {
+    validate_config(cfg);
+    PM_REQUIRE(n > 1, PACMAP_ERR_SAMPLE_SIZE, "Sample size must be larger than one");
+    PM_REQUIRE(x && mlp_params && out_embedding, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    DeviceLock dl(cfg->device);
+    Ctx& c = dl.ctx;
+    const uint64_t dim = cfg->embedding_dimensions;
+    DevBuf<float> dx, dy(c, n * dim), ds;
+    upload(c, dx, x, n * d);
+    const bool snaps = out_snapshots && cfg->snapshots && cfg->n_snapshots > 0;
+    if (snaps) ds.alloc(c, cfg->n_snapshots * n * dim);
+    fit_transform_impl(c, dx.get(), n, d, *cfg, dy.get(), snaps ? ds.get() : nullptr, mlp_params);
+    PM_CUDA(cudaMemcpyAsync(out_embedding, dy.get(), n * dim * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    if (snaps) PM_CUDA(cudaMemcpyAsync(out_snapshots, ds.get(), ds.bytes(), cudaMemcpyDeviceToHost, c.stream));
+    PM_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+pacmap_status pacmap_fit_transform_learned_device(const float* d_x, uint64_t n, uint64_t d, const pacmap_config* cfg,
+                                                  const float* mlp_params, float* d_out_embedding,
+                                                  float* d_out_snapshots) {
+  return guarded([&] {
+    validate_config(cfg);
+    PM_REQUIRE(n > 1, PACMAP_ERR_SAMPLE_SIZE, "Sample size must be larger than one");
+    PM_REQUIRE(d_x && mlp_params && d_out_embedding, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    DeviceLock dl(cfg->device);
+    fit_transform_impl(dl.ctx, d_x, n, d, *cfg, d_out_embedding, d_out_snapshots, mlp_params);
+    PM_CUDA(cudaStreamSynchronize(dl.ctx.stream));
+  });
+}
+
+uint64_t pacmap_mlp_param_count(uint64_t d, uint64_t dim) { return mlp_param_count(d, dim); }
+
+pacmap_status pacmap_mlp_init(uint64_t d, uint64_t dim, uint64_t seed, float* out_params) {
+  return guarded([&] {
+    PM_REQUIRE(out_params != nullptr, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    mlp_init_params(d, dim, seed, out_params);
+  });
+}
+
+pacmap_status pacmap_mlp_train(const float* xp, const float* target, uint64_t n, uint64_t d, uint64_t dim,
+                               uint64_t epochs, uint64_t batch, float lr, float weight_decay, uint64_t seed,
+                               int32_t device, float* inout_params, float* out_epoch_loss) {
+  return guarded([&] {
+    PM_REQUIRE(xp && target && inout_params, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    PM_REQUIRE(dim >= 1 && dim <= 16 && d >= 1 && d <= 4096, PACMAP_ERR_UNSUPPORTED, "MLP supports d <= 4096, dim <= 16");
+    // targets z-scored per dimension: Initialization::Value rescales the output anyway (lib.rs:753-766)
+    std::vector<float> t(target, target + n * dim);
+    for (uint64_t cc = 0; cc < dim; ++cc) {
+      double s = 0.0, s2 = 0.0;
+      for (uint64_t i = 0; i < n; ++i) s += t[i * dim + cc];
+      const double mu = s / static_cast<double>(n);
+      for (uint64_t i = 0; i < n; ++i) s2 += (t[i * dim + cc] - mu) * (t[i * dim + cc] - mu);
+      const double sd = std::sqrt(s2 / static_cast<double>(n)) + 1e-30;
+      for (uint64_t i = 0; i < n; ++i) t[i * dim + cc] = static_cast<float>((t[i * dim + cc] - mu) / sd);
+    }
+    DeviceLock dl(device);
+    Ctx& c = dl.ctx;
+    DevBuf<float> dx, dt;
+    upload(c, dx, xp, n * d);
+    upload(c, dt, t.data(), n * dim);
+    mlp_train_device(c, inout_params, d, dim, dx.get(), dt.get(), n, epochs, batch, lr, weight_decay, seed,
+                     out_epoch_loss);
+  });
+}
+
+pacmap_status pacmap_mlp_apply(const float* params, uint64_t d, uint64_t dim, const float* xp, uint64_t n,
+                               int32_t device, float* out) {
+  return guarded([&] {
+    PM_REQUIRE(params && xp && out, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    DeviceLock dl(device);
+    Ctx& c = dl.ctx;
+    DevBuf<float> dx, dy(c, n * dim);
+    upload(c, dx, xp, n * d);
+    mlp_apply_device(c, params, d, dim, dx.get(), n, dy.get());
+    PM_CUDA(cudaMemcpyAsync(out, dy.get(), dy.bytes(), cudaMemcpyDeviceToHost, c.stream));
+    PM_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+pacmap_status pacmap_mlp_grad(const float* params, uint64_t d, uint64_t dim, const float* xp, const float* target,
+                              uint64_t batch, int32_t device, float* out_grads, float* out_loss) {
+  return guarded([&] {
+    PM_REQUIRE(params && xp && target && out_grads && out_loss, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    DeviceLock dl(device);
+    Ctx& c = dl.ctx;
+    DevBuf<float> dx, dt;
+    upload(c, dx, xp, batch * d);
+    upload(c, dt, target, batch * dim);
+    mlp_grad_device(c, params, d, dim, dx.get(), dt.get(), batch, out_grads, out_loss);
   });
 }
 

@@ -1,0 +1,17 @@
+// The learned initialiser's MLP (d -> 512 -> 512 -> dim), trained and applied on the GPU.
+#pragma once
+#include "engine.cuh"
+
+namespace pacmap {
+// Parameters in the flat host layout [W1 (512 x d), b1 (512), W2 (512 x 512), b2 (512), W3 (dim x 512), b3 (dim)].
+uint64_t mlp_param_count(uint64_t d, uint64_t dim);
+void mlp_init_params(uint64_t d, uint64_t dim, uint64_t seed, float* flat);
+// out (n x dim, device) = MLP(x) for device x (n x d).
+void mlp_apply_device(Ctx& c, const float* params, uint64_t d, uint64_t dim, const float* d_x, uint64_t n, float* d_out);
+// One forward/backward of the mean-squared error on a batch of B rows (device x, t): flat gradients, loss.
+void mlp_grad_device(Ctx& c, const float* params, uint64_t d, uint64_t dim, const float* d_x, const float* d_t,
+                     uint64_t B, float* grads_flat, float* loss);
+// AdamW training on (x, t) rows (device), params updated in place (host flat layout).
+void mlp_train_device(Ctx& c, float* params, uint64_t d, uint64_t dim, const float* d_x, const float* d_t, uint64_t n,
+                      uint64_t epochs, uint64_t batch, float lr, float wd, uint64_t seed, float* epoch_loss);
+}  // namespace pacmap

@@ -25,7 +25,7 @@ from ._abi import ptr
 
 __all__ = [
     "Configuration", "Initialization", "PairConfiguration", "fit_transform", "fit_transform_device",
-    "PaCMapError", "KnnMode", "knn", "quality", "last_launch_count",
+    "PaCMapError", "KnnMode", "knn", "quality", "last_launch_count", "learned",
 ]
 
 # ---------------------------------------------------------------------------------------------
@@ -303,3 +303,4 @@ def last_launch_count() -> int:
 
 from . import knn  # noqa: E402  (submodule mirrors `pacmap::knn`)
 from . import stages  # noqa: E402
+from . import learned  # noqa: E402  (the learned initialiser; no reference counterpart)

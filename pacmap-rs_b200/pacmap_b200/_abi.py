@@ -63,6 +63,13 @@ _SIGS = {
     "pacmap_init_value": (C.c_int, [_vp, _u64, _u64, _i32, _vp]),
     "pacmap_init_random": (C.c_int, [_u64, _u64, _u64, _i32, _vp]),
     "pacmap_quality": (C.c_int, [_vp, _u64, _u64, _vp, _u64, _vp, _u64, _u64, _vp, _u64, _i32, _vp, _vp]),
+    "pacmap_mlp_param_count": (C.c_uint64, [_u64, _u64]),
+    "pacmap_mlp_init": (C.c_int, [_u64, _u64, _u64, _vp]),
+    "pacmap_mlp_train": (C.c_int, [_vp, _vp, _u64, _u64, _u64, _u64, _u64, _f32, _f32, _u64, _i32, _vp, _vp]),
+    "pacmap_mlp_apply": (C.c_int, [_vp, _u64, _u64, _vp, _u64, _i32, _vp]),
+    "pacmap_mlp_grad": (C.c_int, [_vp, _u64, _u64, _vp, _vp, _u64, _i32, _vp, _vp]),
+    "pacmap_fit_transform_learned": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp, _vp]),
+    "pacmap_fit_transform_learned_device": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp, _vp]),
     "pacmap_take_launch_count": (C.c_uint64, []),
     "pacmap_set_stage_timing": (None, [_i32]),
     "pacmap_stage_times": (C.c_uint64, [_vp, _u64]),

@@ -46,10 +46,14 @@ def _rotation(rng, d):
     return q * np.sign(np.diag(r))
 
 
-def anisotropic_mixture(n=1_000_000, d=128, k=50, seed=0, chunk=1 << 16):
+def anisotropic_mixture(n=1_000_000, d=128, k=50, seed=0, chunk=1 << 16, draw_seed=None):
+    """``seed`` fixes the mixture (centres, weights, rotations, scales); ``draw_seed`` (default: the
+    same stream) the points drawn from it, so two draw seeds give fresh samples of one generator."""
     rng = np.random.default_rng(seed)
+    rd = rng if draw_seed is None else np.random.default_rng(draw_seed)
     centres = rng.normal(0.0, 4.0, size=(k, d))
-    sizes = rng.multinomial(n, rng.dirichlet(np.full(k, 2.0)))
+    weights = rng.dirichlet(np.full(k, 2.0))
+    sizes = rd.multinomial(n, weights)
     x = np.empty((n, d), np.float32)
     labels = np.empty(n, np.int32)
     row = 0
@@ -60,11 +64,11 @@ def anisotropic_mixture(n=1_000_000, d=128, k=50, seed=0, chunk=1 << 16):
         m = int(sizes[c])
         for s in range(0, m, chunk):
             e = min(m, s + chunk)
-            z = rng.normal(size=(e - s, d))
+            z = rd.normal(size=(e - s, d))
             x[row + s:row + e] = (centres[c] + z @ a.T).astype(np.float32)
         labels[row:row + m] = c
         row += m
-    perm = rng.permutation(n)
+    perm = rd.permutation(n)
     return x[perm], labels[perm]
 
 

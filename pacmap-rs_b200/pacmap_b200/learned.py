@@ -1,0 +1,103 @@
+"""The learned initialiser: an MLP d -> 512 -> 512 -> dim from preprocessed data to an embedding.
+
+No counterpart in beamform/pacmap-rs. The reference accepts any starting embedding through
+``Initialization::Value`` (src/lib.rs:753-766, z-scored to std 1e-4); this module trains a network on
+the (x, embedding) pairs that a plain fit produces for one data generator, and starts new fits of the
+same generator from its prediction, so that a shortened schedule (``SHORT_SCHEDULE``) replaces the
+plain one (``PLAIN_SCHEDULE``). Training, inference and the gradient check all run on the GPU
+(tcgen05 BF16 GEMMs with FP32 accumulation, AdamW) through the C ABI (include/pacmap.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Optional
+
+import numpy as np
+
+from . import Configuration, Initialization, _abi, _check, _CConfig
+from ._abi import ptr
+
+PLAIN_SCHEDULE = (100, 100, 250)
+SHORT_SCHEDULE = (0, 50, 150)
+HIDDEN = 512
+
+
+def param_count(d: int, dim: int) -> int:
+    return int(_abi.lib().pacmap_mlp_param_count(d, dim))
+
+
+def init_params(d: int, dim: int, seed: int = 0) -> np.ndarray:
+    """Seeded U(-1/sqrt(fan_in), 1/sqrt(fan_in)) parameters in the flat layout
+    [W1 (512 x d), b1, W2 (512 x 512), b2, W3 (dim x 512), b3]."""
+    p = np.zeros(param_count(d, dim), np.float32)
+    _check(_abi.lib().pacmap_mlp_init(d, dim, seed & (2**64 - 1), ptr(p)))
+    return p
+
+
+def train(params, xp, target, epochs: int = 20, batch: int = 4096, lr: float = 1e-3, weight_decay: float = 1e-4,
+          seed: int = 0, device: int = 0):
+    """AdamW on the mean-squared error between MLP(xp) and the per-dimension z-scored target.
+
+    Returns (trained parameters, loss of each epoch)."""
+    xp = np.ascontiguousarray(xp, dtype=np.float32)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    n, d = xp.shape
+    dim = t.shape[1]
+    p = np.array(params, dtype=np.float32, copy=True)
+    assert p.size == param_count(d, dim), "parameter count does not match (d, dim)"
+    losses = np.zeros(max(epochs, 1), np.float32)
+    _check(_abi.lib().pacmap_mlp_train(ptr(xp), ptr(t), n, d, dim, epochs, batch, lr, weight_decay,
+                                       seed & (2**64 - 1), device, ptr(p), ptr(losses)))
+    return p, losses[:epochs]
+
+
+def apply(params, xp, dim: int, device: int = 0) -> np.ndarray:
+    """MLP(xp) (n x dim)."""
+    xp = np.ascontiguousarray(xp, dtype=np.float32)
+    n, d = xp.shape
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    out = np.zeros((n, dim), np.float32)
+    _check(_abi.lib().pacmap_mlp_apply(ptr(p), d, dim, ptr(xp), n, device, ptr(out)))
+    return out
+
+
+def gradient(params, xp, target, device: int = 0):
+    """(loss, flat gradient) of the mean-squared error on one batch (rows a multiple of 128)."""
+    xp = np.ascontiguousarray(xp, dtype=np.float32)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    B, d = xp.shape
+    dim = t.shape[1]
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    g = np.zeros(p.size, np.float32)
+    loss = C.c_float(0)
+    _check(_abi.lib().pacmap_mlp_grad(ptr(p), d, dim, ptr(xp), ptr(t), B, device, ptr(g), C.byref(loss)))
+    return loss.value, g
+
+
+def fit_transform_learned(x, params, config: Optional[Configuration] = None):
+    """fit_transform (lib.rs:294-367) starting from MLP(x') through Initialization::Value.
+
+    ``config.initialization`` is ignored; pass a shortened ``num_iters`` (``SHORT_SCHEDULE``)."""
+    config = config or dataclasses.replace(Configuration(), num_iters=SHORT_SCHEDULE)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    n, d = x.shape
+    dim = int(config.embedding_dimensions)
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    cc = _CConfig(dataclasses.replace(config, initialization=Initialization.Random(0)), n)
+    out = np.zeros((n, dim), np.float32)
+    snaps = None
+    if config.snapshots is not None:
+        snaps = np.zeros((len(config.snapshots), n, dim), np.float32)
+    _check(_abi.lib().pacmap_fit_transform_learned(ptr(x), n, d, C.byref(cc.c), ptr(p), ptr(out), ptr(snaps)))
+    return out, snaps
+
+
+def fit_transform_learned_device(x_ptr: int, n: int, d: int, out_ptr: int, params, config: Configuration,
+                                 snapshots_ptr: Optional[int] = None) -> None:
+    """fit_transform_learned on device memory (raw CUDA pointers); params stay a host array."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    cc = _CConfig(dataclasses.replace(config, initialization=Initialization.Random(0)), n)
+    _check(_abi.lib().pacmap_fit_transform_learned_device(C.c_void_p(x_ptr), n, d, C.byref(cc.c), ptr(p),
+                                                          C.c_void_p(out_ptr),
+                                                          C.c_void_p(snapshots_ptr) if snapshots_ptr else None))
