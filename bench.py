@@ -2,11 +2,17 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n ROWS] [--d COLS]
 
-One step = one full fit_transform (preprocess -> exact kNN -> reselection -> MN/FP sampling -> CSR ->
-450 fused gradient+Adam iterations in one CUDA graph) of the whole synthetic dataset:
-  * value: inputs resident in HBM, C ABI `pacmap_fit_transform_device`, CUDA events around each step;
-  * e2e:   the same through `pacmap_fit_transform` with pinned host input and host output (the host
-           copies are inside the timed region).
+A learned initialiser (MLP 128-512-512-2) is first trained, outside the timed region, on the plain GPU
+embedding of 200,000 draws of the generator. One step = one full learned-init fit_transform of a fresh
+draw (preprocess -> exact kNN -> reselection -> MN/FP sampling -> MLP prediction as Value init -> CSR ->
+the shortened schedule (0, 50, 150) of fused gradient+Adam iterations in one CUDA graph):
+  * value: inputs resident in HBM, C ABI `pacmap_fit_transform_learned_device`, CUDA events around
+           each step; the plain schedule (Random init, (100, 100, 250)) on the same draw is timed the
+           same way (`plain_gpu_s`), and both embeddings are judged by 10-NN preservation and triplet
+           accuracy; a learned run more than 0.005 below the plain preservation continues on the plain
+           schedule, inside the timed step;
+  * e2e:   the learned step through `pacmap_fit_transform_learned` with pinned host input and host
+           output (the host copies are inside the timed region).
 With N GPUs (torchrun) every rank embeds its own dataset (replicas only: the path does not shard);
 timing is the max over ranks and value is seconds per embedding for the whole job.
 `--impl reference` times the CPU restatement of the reference (the reference's Rust crate cannot be
@@ -84,13 +90,11 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def make_data(n, d, seed):
+def make_data(n, d, seed, draw_seed=None):
+    """n draws of the anisotropic 50-Gaussian mixture fixed by `seed` (fresh points per `draw_seed`)."""
     from pacmap_b200 import datasets
 
-    if d == 128:
-        x, _ = datasets.anisotropic_mixture(n=n, d=d, k=50, seed=seed)
-    else:
-        x, _ = datasets.isotropic_mixture(n=n, d=d, k=50, seed=seed)
+    x, _ = datasets.anisotropic_mixture(n=n, d=d, k=50, seed=seed, draw_seed=draw_seed)
     return x
 
 
@@ -150,10 +154,23 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _optimize_bytes(n, dim, iters, k=10, n_mn=5, n_fp=20):
+    """Algorithmic HBM bytes of the gradient + Adam iterations: 8 B per active pair (its two u32
+    endpoints, read once), 4*n*dim for y read by the gradient, 24*n*dim for Adam (y, m, v read+write);
+    mid-near pairs are inactive in phase 3 (w_mn = 0)."""
+    p12 = n * (k + n_mn + n_fp)
+    p3 = n * (k + n_fp)
+    per = lambda pairs: 8 * pairs + 28 * n * dim  # noqa: E731
+    return (iters[0] + iters[1]) * per(p12) + iters[2] * per(p3)
+
+
 def run_ours(args, rank, world, local_rank):
+    import ctypes as C
+
     import torch
 
     import pacmap_b200 as pm
+    from pacmap_b200 import _abi, datasets, learned
 
     torch.cuda.set_device(local_rank)
     dist = world > 1
@@ -163,27 +180,55 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as tdist
 
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    n, d = args.n, args.d
-    x = make_data(n, d, seed=rank)
-    cfg = config_for(pm, 0)
-    cfg.device = local_rank
-    dx = torch.from_numpy(x).to(f"cuda:{local_rank}")
-    dy = torch.empty((n, 2), dtype=torch.float32, device=f"cuda:{local_rank}")
+    n, d, dim = args.n, args.d, 2
+    n_train = min(200_000, max(n // 5, 4096))
+    # the learned initialiser is trained once per generator (outside the timed region): plain GPU PaCMAP
+    # of n_train draws, then AdamW on (x', embedding)
+    train_s, train_losses = None, None
+    if args.minimal:
+        params = learned.init_params(d, dim, seed=0)
+    else:
+        x_train = make_data(n_train, d, seed=0, draw_seed=10_000 + rank)
+        y_train, _ = pm.fit_transform(x_train, pm.Configuration(initialization=pm.Initialization.Random(7), seed=7,
+                                                                device=local_rank))
+        xp_train, *_ = pm.stages.preprocess(x_train, local_rank)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        params, train_losses = learned.train(learned.init_params(d, dim, seed=0), xp_train, y_train, epochs=20,
+                                             batch=4096, lr=1e-3, weight_decay=1e-4, seed=0, device=local_rank)
+        train_s = time.perf_counter() - t0
+        del x_train, y_train, xp_train
+    # a fresh draw of the same generator
+    x = make_data(n, d, seed=0, draw_seed=1000 + rank)
+    cfg_plain = pm.Configuration(initialization=pm.Initialization.Random(7), seed=7, device=local_rank)
+    cfg_short = pm.Configuration(seed=7, num_iters=learned.SHORT_SCHEDULE, device=local_rank)
+    dev = f"cuda:{local_rank}"
+    dx = torch.from_numpy(x).to(dev)
+    dy_l = torch.empty((n, dim), dtype=torch.float32, device=dev)
+    dy_p = torch.empty((n, dim), dtype=torch.float32, device=dev)
+    dy_c = torch.empty((n, dim), dtype=torch.float32, device=dev)
     hx = torch.from_numpy(x).pin_memory()
-    hy = torch.empty((n, 2), dtype=torch.float32).pin_memory()
+    hy = torch.empty((n, dim), dtype=torch.float32).pin_memory()
+    gate = {"continued": False}
 
-    def step_device():
-        pm.fit_transform_device(dx.data_ptr(), n, d, dy.data_ptr(), cfg)
+    def step_learned():
+        learned.fit_transform_learned_device(dx.data_ptr(), n, d, dy_l.data_ptr(), params, cfg_short)
+        if gate["continued"]:
+            # the run missed the plain run's 10-NN preservation by more than 0.005: continue it on the
+            # plain schedule from where it stopped
+            cont = pm.Configuration(initialization=pm.Initialization.Value(dy_l.cpu().numpy()), seed=7,
+                                    device=local_rank)
+            pm.fit_transform_device(dx.data_ptr(), n, d, dy_c.data_ptr(), cont)
+
+    def step_plain():
+        pm.fit_transform_device(dx.data_ptr(), n, d, dy_p.data_ptr(), cfg_plain)
 
     def step_e2e():
-        import ctypes as C
-
-        from pacmap_b200 import _abi
-
-        cc = pm._CConfig(cfg, n)
-        rc = _abi.lib().pacmap_fit_transform(C.c_void_p(hx.data_ptr()), n, d, C.byref(cc.c),
-                                             C.c_void_p(hy.data_ptr()), None)
-        pm._check(rc)
+        cc = pm._CConfig(cfg_short, n)
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        pm._check(_abi.lib().pacmap_fit_transform_learned(C.c_void_p(hx.data_ptr()), n, d, C.byref(cc.c),
+                                                          C.c_void_p(p.ctypes.data), C.c_void_p(hy.data_ptr()),
+                                                          None))
 
     def barrier():
         if dist:
@@ -201,38 +246,48 @@ def run_ours(args, rank, world, local_rank):
         ms = ev0.elapsed_time(ev1)
         barrier()
         if dist:
-            t = torch.tensor([ms], device=f"cuda:{local_rank}")
+            t = torch.tensor([ms], device=dev)
             tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
             ms = float(t.item())
         return ms
 
     for _ in range(args.warmup):
-        step_device()
-    stages = {}
-    if not args.minimal:
-        # stage breakdown of one untimed step (CUDA events inside the library, on its stream)
-        pm.set_stage_timing(True)
-        step_device()
-        stages = pm.stage_times()
-        pm.set_stage_timing(False)
-    pm.last_launch_count()
-    with ClockSampler(local_rank) as clk:
-        ms = timed(step_device, args.steps)
-    launches = pm.last_launch_count()
+        step_learned()
     if args.minimal:
+        pm.last_launch_count()
+        ms = timed(step_learned, args.steps)
+        launches = pm.last_launch_count()
         if rank == 0:
             print(json.dumps({"minimal": True, "ms_per_step": ms / args.steps, "gpu_launches": launches}), flush=True)
         if dist:
             tdist.destroy_process_group()
         return
+    for _ in range(args.warmup):
+        step_plain()
+    # quality gate: learned (short schedule) against the plain schedule on the same draw
+    sample, trip = datasets.quality_sample(n, 10000, 5)
+    q_plain = pm.quality(x, dy_p.cpu().numpy(), sample, trip, 10, local_rank)
+    q_learned = pm.quality(x, dy_l.cpu().numpy(), sample, trip, 10, local_rank)
+    gate["continued"] = q_learned[0] < q_plain[0] - 0.005
+    q_final = q_learned
+    if gate["continued"]:
+        step_learned()
+        q_final = pm.quality(x, dy_c.cpu().numpy(), sample, trip, 10, local_rank)
+    # stage breakdown of one untimed step of each (CUDA events inside the library, on its stream)
+    pm.set_stage_timing(True)
+    step_plain()
+    stages_plain = pm.stage_times()
+    learned.fit_transform_learned_device(dx.data_ptr(), n, d, dy_l.data_ptr(), params, cfg_short)
+    stages_learned = pm.stage_times()
+    pm.set_stage_timing(False)
+
+    pm.last_launch_count()
+    with ClockSampler(local_rank) as clk:
+        ms = timed(step_learned, args.steps)
+    launches = pm.last_launch_count()
+    ms_plain = timed(step_plain, args.steps)
     e2e_steps = max(1, args.steps // 2)
     ms_e2e = timed(step_e2e, e2e_steps)
-
-    # quality of the embedding (outside the timed region)
-    from pacmap_b200 import datasets
-
-    sample, trip = datasets.quality_sample(n, 10000, 5)
-    pres, tacc = pm.quality(x, dy.cpu().numpy(), sample, trip, 10, local_rank)
 
     if rank != 0:
         if dist:
@@ -240,26 +295,47 @@ def run_ours(args, rank, world, local_rank):
         return
     hbm, bf16, src = _peaks()
     per_step = ms / args.steps
-    knn_ms = stages.get("knn_filter") or stages.get("knn", 0.0)
+    per_plain = ms_plain / args.steps
+    knn_ms = stages_learned.get("knn_filter") or stages_learned.get("knn", 0.0)
     flops = 2.0 * n * n * d
     achieved_tf = flops / (knn_ms * 1e-3) / 1e12 if knn_ms > 0 else None
+    opt_ms = stages_learned.get("optimize", 0.0)
+    opt_bytes = _optimize_bytes(n, dim, learned.SHORT_SCHEDULE)
+    opt_gbs = opt_bytes / (opt_ms * 1e-3) / 1e9 if opt_ms > 0 else None
+    rnd = lambda q: {"knn10_preservation": round(q[0], 5), "triplet_accuracy": round(q[1], 4)}  # noqa: E731
     line = {
         "metric": METRIC, "value": round(per_step / 1000.0 / world, 4), "unit": "s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"plain PaCMAP {n}x{d} -> 2-D, Random init, 450 iterations, exact kNN (k'={min(40 + 50, n - 1)})",
-                   "n": n, "d": d, "generator": "anisotropic 50-Gaussian mixture" if d == 128 else "isotropic mixture",
+        "config": {"workload": (f"learned-init PaCMAP of a fresh {n}x{d} draw -> 2-D: MLP {d}-512-512-2 prediction "
+                                f"as Value init + schedule {learned.SHORT_SCHEDULE}; vs plain Random(7) with "
+                                f"{learned.PLAIN_SCHEDULE}; exact kNN (k'={min(40 + 50, n - 1)})"),
+                   "n": n, "d": d, "generator": "anisotropic 50-Gaussian mixture (seed 0; draw seed 1000+rank)",
+                   "mlp_training": f"{n_train} draws (draw seed 10000+rank), plain GPU embedding, 20 epochs, batch "
+                                   "4096, AdamW lr 1e-3 wd 1e-4 (outside the timed region)",
                    "l2": "inputs larger than L2 (x = %.0f MB)" % (n * d * 4 / 1e6), "parallelism": f"replicas{world}",
-                   "init": "Random(7)", "knn_mode": "auto"},
+                   "knn_mode": "auto"},
+        "plain_gpu_s": round(per_plain / 1000.0 / world, 4),
+        "learned_over_plain": round(per_step / per_plain, 4),
+        "gate": {"rule": "continue on the plain schedule if 10-NN preservation < plain - 0.005",
+                 "continued": gate["continued"], "plain": rnd(q_plain), "learned_short": rnd(q_learned),
+                 "final": rnd(q_final)},
+        "mlp_train_s": round(train_s, 3) if train_s else None,
+        "mlp_train_loss": [round(float(v), 4) for v in (train_losses[0], train_losses[-1])] if train_losses is not None else None,
         "e2e": {"value": round(ms_e2e / e2e_steps / 1000.0 / world, 4), "unit": "s",
-                "h2d_bytes_per_step": int(n * d * 4), "d2h_bytes_per_step": int(n * 2 * 4)},
+                "h2d_bytes_per_step": int(n * d * 4 + np.asarray(params).nbytes), "d2h_bytes_per_step": int(n * dim * 4)},
         "gpu_launches": int(launches),
-        "stages_ms": {k: round(v, 3) for k, v in stages.items()},
-        "quality": {"knn10_preservation": round(pres, 4), "triplet_accuracy": round(tacc, 4)},
-        "roofline": {"kernel": "knn_filter_kernel (tcgen05 distance GEMM + fused candidate filter)" if stages.get("knn_filter") else "knn_simt_kernel", "bound": "tensor",
+        "stages_ms": {"learned": {k: round(v, 3) for k, v in stages_learned.items()},
+                      "plain": {k: round(v, 3) for k, v in stages_plain.items()}},
+        "roofline": {"kernel": "knn_filter_kernel (tcgen05 distance GEMM + fused candidate filter)" if stages_learned.get("knn_filter") else "knn_simt_kernel", "bound": "tensor",
                      "achieved": round(achieved_tf, 2) if achieved_tf else None, "peak": bf16, "unit": "TFLOP/s",
                      "frac": round(achieved_tf / bf16, 4) if achieved_tf else None, "traffic": None,
                      "peak_source": f"{src} bf16 dense", "algorithmic": "2*n^2*d flops per launch"},
+        "roofline_optimizer": {"kernel": "grad_adam_kernel (CSR gradient + Adam, CUDA graph)", "bound": "hbm",
+                               "achieved": round(opt_gbs, 1) if opt_gbs else None, "peak": hbm, "unit": "GB/s",
+                               "frac": round(opt_gbs / hbm, 4) if opt_gbs else None,
+                               "algorithmic": "8 B per active pair + 28*n*dim B per iteration",
+                               "peak_source": f"{src} HBM copy"},
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:

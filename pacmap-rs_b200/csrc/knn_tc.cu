@@ -47,6 +47,7 @@ constexpr int TC_THREADS = 320;    // warp 0 TMA, warp 1 MMA + TMEM owner, warps
 constexpr int TC_EPI_WARPS = 8;
 constexpr int TC_TMEM_COLS = 512;  // 2 accumulator stages x 2 halves x 128 columns
 constexpr int KB_BYTES = 128 * 128;  // one 128-row x 64-element (128 B) swizzled K block
+constexpr int G_BYTES = 128 * 32;    // one 128-row x 16-element (32 B) column-term tile
 
 struct alignas(8) TcShared {
   uint64_t full[TC_STAGES];
@@ -419,23 +420,49 @@ __global__ void split_rows_kernel(const float* __restrict__ x, const uint32_t* _
 // e_j and the per-column/per-row constants of the filter. Slack factors: the f32 sums of n, A, B
 // are inflated by 2^-16 relative; gamma covers the reference's own f32 distance sum, every f32
 // rounding of the epilogue and of these constants.
+//
+// The filter's accumulator starts at -g_j / 2 (a rank-1 MMA: ones x the column term gq) and adds
+// h_i . h_j on top, so its rounding also sees the column term: every one of the S = KP/16 + 1 MMA steps
+// may lose 17 * 2^-21 of the largest magnitude in the sum, |g_j|/2 + sum_k |h_ik h_jk|; the column
+// part goes to e_j, the product part is split by AM-GM like eta. gq[j] stores -g_j / 4 as three bf16
+// parts with an exact sum, twice (elements 0..2 and 8..10, zero elsewhere), so that the all-ones row
+// operand sums them to -g_j / 2 whatever the swizzle order of the two 16-byte halves.
 __global__ void bound_kernel(uint64_t n, uint64_t n_pad, int d, int KP, float rho, const float* __restrict__ nrm,
-                             const float* __restrict__ A, const float* __restrict__ B, float2* __restrict__ ge) {
+                             const float* __restrict__ A, const float* __restrict__ B, float2* __restrict__ ge,
+                             uint16_t* __restrict__ gq) {
   const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (j >= n_pad) return;
+  uint16_t parts[3] = {0, 0, 0};
   if (j >= n) {
     ge[j] = make_float2(__int_as_float(0x7f800000), 0.0f);  // +inf: padding columns never pass
-    return;
+    parts[0] = 0xFF80u;                                       // bf16 -inf: D = -inf, v = +inf
+  } else {
+    const float infl = 1.0f + 1.52587890625e-05f;  // 1 + 2^-16
+    const float a = A[j] * infl, b = B[j] * infl, nn = nrm[j] * infl;
+    const float eta = static_cast<float>(KP) * 4.76837158203125e-07f;                  // K * 2^-21
+    const float eta_s = static_cast<float>(KP / 16 + 1) * 17.0f * 4.76837158203125e-07f;  // S * 17 * 2^-21
+    // f32 sums of n (d terms), the reference's own distance sum (d/8 + 8 terms, on D <= 2(n_i + n_j)),
+    // and the epilogue's roundings: (2d + 64) 2^-24 + 2^-19.
+    const float gamma = static_cast<float>(2 * d + 64) * 5.9604644775390625e-08f + 1.9073486328125e-06f;
+    const float e0 = 0.5f * (rho * a + b / rho) + 0.5f * b + 0.5f * eta * a + gamma * nn;
+    const float e = e0 + 0.5f * eta_s * a + 0.5f * eta_s * (nn + 4.0f * e0) + 1e-30f;
+    const float e_safe = e * (1.0f + 9.765625e-04f);  // 2^-10 relative margin on the bound itself
+    const float g = nrm[j] - 2.0f * e_safe;
+    ge[j] = make_float2(g, 4.0f * e_safe);
+    const float q = -0.25f * g;
+    const __nv_bfloat16 p0 = __float2bfloat16_rn(q);
+    const float r1 = q - __bfloat162float(p0);
+    const __nv_bfloat16 p1 = __float2bfloat16_rn(r1);
+    const __nv_bfloat16 p2 = __float2bfloat16_rn(r1 - __bfloat162float(p1));
+    parts[0] = __bfloat16_as_ushort(p0);
+    parts[1] = __bfloat16_as_ushort(p1);
+    parts[2] = __bfloat16_as_ushort(p2);
   }
-  const float infl = 1.0f + 1.52587890625e-05f;  // 1 + 2^-16
-  const float a = A[j] * infl, b = B[j] * infl, nn = nrm[j] * infl;
-  const float eta = static_cast<float>(KP) * 4.76837158203125e-07f;                   // K * 2^-21
-  // f32 sums of n (d terms), the reference's own distance sum (d/8 + 8 terms, on D <= 2(n_i + n_j)),
-  // and the epilogue's roundings: (2d + 64) 2^-24 + 2^-19.
-  const float gamma = static_cast<float>(2 * d + 64) * 5.9604644775390625e-08f + 1.9073486328125e-06f;
-  const float e = 0.5f * (rho * a + b / rho) + 0.5f * b + 0.5f * eta * a + gamma * nn + 1e-30f;
-  const float e_safe = e * (1.0f + 9.765625e-04f);  // 2^-10 relative margin on the bound itself
-  ge[j] = make_float2(nrm[j] - 2.0f * e_safe, 4.0f * e_safe);
+  uint4 w[2];
+  w[0] = make_uint4(parts[0] | (static_cast<uint32_t>(parts[1]) << 16), parts[2], 0u, 0u);
+  w[1] = w[0];
+  reinterpret_cast<uint4*>(gq + j * 16)[0] = w[0];
+  reinterpret_cast<uint4*>(gq + j * 16)[1] = w[1];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -443,22 +470,30 @@ __global__ void bound_kernel(uint64_t n, uint64_t n_pad, int d, int KP, float rh
 // ---------------------------------------------------------------------------------------------
 template <int KB, int PER>  // K blocks of 64 elements: KP = 64 * KB; candidate buffer C = 32 * PER
 __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
-    const __grid_constant__ CUtensorMap hmap, uint64_t n, uint64_t n_pad, uint32_t idesc, const float2* __restrict__ ge,
-    const float* __restrict__ nrm, const uint32_t* __restrict__ perm, int rank, uint32_t* __restrict__ cand_idx,
-    float* __restrict__ cand_v, float* __restrict__ cand_u, int* __restrict__ cand_cnt, uint32_t* __restrict__ overflow_rows,
-    uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err) {
+    const __grid_constant__ CUtensorMap hmap, const __grid_constant__ CUtensorMap gmap, uint64_t n, uint64_t n_pad,
+    uint32_t idesc, const float2* __restrict__ ge, const float* __restrict__ nrm, const uint32_t* __restrict__ perm,
+    int rank, uint32_t* __restrict__ cand_idx, float* __restrict__ cand_v, float* __restrict__ cand_u,
+    int* __restrict__ cand_cnt, uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow,
+    uint32_t* __restrict__ err) {
   constexpr int C = 32 * PER;
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-  // 1024-byte aligned operand region: A [2 halves][KB][16 KB], B [STAGES][KB][16 KB], then TcShared.
+  // 1024-byte aligned operand region: A [2 halves][KB][16 KB], the all-ones tile [4 KB], the
+  // column-term tiles [STAGES][4 KB], B [STAGES][KB][16 KB], then TcShared (the small tiles sit below
+  // the large B stages).
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* a_smem = base;
-  unsigned char* b_smem = base + 2 * KB * KB_BYTES;
+  unsigned char* one_smem = base + 2 * KB * KB_BYTES;
+  unsigned char* g_smem = one_smem + G_BYTES;
+  unsigned char* b_smem = g_smem + TC_STAGES * G_BYTES;
   TcShared* sh = reinterpret_cast<TcShared*>(b_smem + TC_STAGES * KB * KB_BYTES);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t row0 = static_cast<uint64_t>(blockIdx.x) * TC_BM;
   const int ntiles = static_cast<int>(n_pad / TC_BN);
 
+  // A operand of the column-term MMA: bf16 1.0 in every element (every swizzle reads the same tile).
+  for (int e = threadIdx.x; e < G_BYTES / 4; e += TC_THREADS) reinterpret_cast<uint32_t*>(one_smem)[e] = 0x3F803F80u;
+  fence_proxy_async_smem();
   if (threadIdx.x == 0) {
     for (int s = 0; s < TC_STAGES; ++s) {
       mbar_init(&sh->full[s], 1);
@@ -495,10 +530,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
       for (int t = 0; t < ntiles; ++t) {
         const int s = t % TC_STAGES;
         if (t >= TC_STAGES && !mbar_wait(&sh->empty[s], ((t / TC_STAGES) + 1) & 1, abort_flag)) break;
-        mbar_expect_tx(&sh->full[s], KB * KB_BYTES);
+        mbar_expect_tx(&sh->full[s], KB * KB_BYTES + G_BYTES);
         const int tile = sweep_tile(t, static_cast<int>(blockIdx.x), ntiles);
         for (int kb = 0; kb < KB; ++kb)
           tma_load_2d(b_smem + (s * KB + kb) * KB_BYTES, &hmap, &sh->full[s], kb * 64, tile * TC_BN);
+        tma_load_2d(g_smem + s * G_BYTES, &gmap, &sh->full[s], 0, tile * TC_BN);
         issued = t + 1;
       }
       if (issued < ntiles) {
@@ -517,7 +553,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     // ------------------------------- MMA issuer -------------------------------
     if (lane == 0) {
       bool ok = mbar_wait(&sh->a_full, 0, abort_flag);
-      const uint32_t a_addr = smem_u32(a_smem), b_addr = smem_u32(b_smem);
+      const uint32_t a_addr = smem_u32(a_smem), b_addr = smem_u32(b_smem), g_addr = smem_u32(g_smem);
+      const uint64_t ones = sdesc_sw32(smem_u32(one_smem));
+      const uint32_t idesc_col = idesc_f16(true);  // the column term is bf16 x bf16
       int t = 0;
       for (; ok && t < ntiles; ++t) {
         const int s = t % TC_STAGES, acc = t & 1;
@@ -530,16 +568,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
           break;
         }
         tc_fence_after();
+        const uint64_t gd = sdesc_sw32(g_addr + s * G_BYTES);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const uint32_t d_tmem = tmem + acc * 256 + h * 128;
+          // D = -g_j / 2 (rank-1: ones x the column term), then D += h_i . h_j
+          umma_f16(d_tmem, ones, gd, idesc_col, 0u);
 #pragma unroll
           for (int kb = 0; kb < KB; ++kb) {
             const uint64_t ad = sdesc_sw128(a_addr + (h * KB + kb) * KB_BYTES);
             const uint64_t bd = sdesc_sw128(b_addr + (s * KB + kb) * KB_BYTES);
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-              umma_f16(d_tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) ? 1u : 0u);
+            for (int kk = 0; kk < 4; ++kk) umma_f16(d_tmem, ad + 2 * kk, bd + 2 * kk, idesc, 1u);
           }
         }
         umma_commit(&sh->empty[s]);
@@ -557,6 +597,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     }
   } else {
     // ------------------------------- epilogue (8 warps) -------------------------------
+    // The accumulator holds D = h_i . h_j - g_j / 2, so v_ij = g_j - 2 G_ij = -2 D exactly; a
+    // column passes when v <= theta. Each 32-column group is screened by its maximum D first.
     const int ew = warp - 2;
     const int half = ew >> 2;
     const int quad = warp & 3;  // TMEM lane quadrant this warp may access
@@ -569,6 +611,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const float e4_i = valid ? ge[row].y : 0.0f;
     const uint64_t cbase = row * static_cast<uint64_t>(C);
     bool ok = true;
+    auto screen = [&](const uint32_t (&r)[32], int colb) {
+      float m8[4];
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        const float* D = reinterpret_cast<const float*>(r) + 8 * g;
+        m8[g] = fmax3(fmax3(D[0], D[1], D[2]), fmax3(D[3], D[4], D[5]), fmaxf(D[6], D[7]));
+      }
+      const float m = fmaxf(fmax3(m8[0], m8[1], m8[2]), m8[3]);
+      if (__any_sync(0xFFFFFFFFu, -2.0f * m <= theta)) {
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          if (__any_sync(0xFFFFFFFFu, -2.0f * m8[g] <= theta)) {
+#pragma unroll
+            for (int c = 8 * g; c < 8 * g + 8; ++c) {
+              const float v = -2.0f * __uint_as_float(r[c]);
+              if (v <= theta) {
+                const int col = colb + c;
+                cand_idx[cbase + cnt] = static_cast<uint32_t>(col);
+                cand_v[cbase + cnt] = v;
+                cand_u[cbase + cnt] = v + __ldg(&ge[col].y);
+                ++cnt;
+              }
+            }
+          }
+        }
+      }
+    };
     for (int t = 0; t < ntiles; ++t) {
       const int acc = t & 1;
       if (!mbar_wait(&sh->tmem_full[acc], (t >> 1) & 1, abort_flag)) {
@@ -578,43 +647,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
       tc_fence_after();
       const int col0 = sweep_tile(t, static_cast<int>(blockIdx.x), ntiles) * TC_BN;
       const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) + acc * 256 + half * 128;
-      // The next tile's column constants go to L1 now (8 x 128 B of (g, 4e) pairs).
-      if (lane < 8 && t + 1 < ntiles)
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(ge + sweep_tile(t + 1, static_cast<int>(blockIdx.x), ntiles) * TC_BN +
-                                                        lane * 16));
 #pragma unroll 1
-      for (int ch = 0; ch < 4; ++ch) {
-        // column constants first: their loads are in flight while the accumulator is read from TMEM
-        const float4* gp = reinterpret_cast<const float4*>(ge + col0 + ch * 32);
-        float4 gq[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) gq[q] = __ldg(gp + q);
-        float G[32];
-        tmem_ld32(taddr + ch * 32, G);
-        float v[32];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          v[2 * q + 0] = fmaf(-2.0f, G[2 * q + 0], gq[q].x);
-          v[2 * q + 1] = fmaf(-2.0f, G[2 * q + 1], gq[q].z);
-        }
-        // Warp-uniform early-outs per 8 columns; an insertion is three plain stores.
-#pragma unroll
-        for (int o = 0; o < 32; o += 8) {
-          const float m8 = fminf(fminf(fminf(v[o], v[o + 1]), fminf(v[o + 2], v[o + 3])),
-                                 fminf(fminf(v[o + 4], v[o + 5]), fminf(v[o + 6], v[o + 7])));
-          if (__any_sync(0xFFFFFFFFu, m8 <= theta)) {
-#pragma unroll
-            for (int c = o; c < o + 8; ++c) {
-              if (v[c] <= theta) {
-                const float e4j = (c & 1) ? gq[c >> 1].w : gq[c >> 1].y;
-                cand_idx[cbase + cnt] = static_cast<uint32_t>(col0 + ch * 32 + c);
-                cand_v[cbase + cnt] = v[c];
-                cand_u[cbase + cnt] = v[c] + e4j;
-                ++cnt;
-              }
-            }
-          }
-        }
+      for (int cp = 0; cp < 2; ++cp) {  // 64 columns per pass, two TMEM loads in flight
+        uint32_t r0[32], r1[32];
+        tmem_ld32_issue(taddr + cp * 64, r0);
+        tmem_ld32_issue(taddr + cp * 64 + 32, r1);
+        tmem_wait_ld_tied(r0);
+        tie_regs(r1);
+        screen(r0, col0 + cp * 64);
+        screen(r1, col0 + cp * 64 + 32);
       }
       tc_fence_before();
       __syncwarp();
@@ -780,6 +821,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   DevBuf<uint16_t> H(c, n_pad * KP);
   DevBuf<float> nrm(c, n_pad), A(c, n_pad), B(c, n_pad);
   DevBuf<float2> ge(c, n_pad);
+  DevBuf<uint16_t> gq(c, n_pad * 16);
   const unsigned sgrid = std::min<unsigned>(ceil_div(n_pad, 8), c.sm_count * 8);
   DevBuf<double> partial(c, 2 * sgrid);
   if (bf16)
@@ -799,7 +841,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   }
   const float rho = (sa > 0.0 && sb > 0.0) ? static_cast<float>(std::sqrt(sb / sa)) : 1e-4f;
   bound_kernel<<<ceil_div(n_pad, 256), 256, 0, c.stream>>>(n, n_pad, static_cast<int>(d), KP, rho, nrm.get(), A.get(),
-                                                          B.get(), ge.get());
+                                                          B.get(), ge.get(), gq.get());
   PM_LAUNCHED();
 
   CUtensorMap map;
@@ -813,6 +855,16 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
                                       CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   PM_REQUIRE(cr == CUDA_SUCCESS, PACMAP_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(cr));
+  // the column term: [n_pad][16] bf16, box 16 x 128, 32-byte swizzle (x is always 0)
+  CUtensorMap gmap;
+  std::memset(&gmap, 0, sizeof(gmap));
+  const cuuint64_t gdims[2] = {16, static_cast<cuuint64_t>(n_pad)};
+  const cuuint64_t gstrides[1] = {32};
+  const cuuint32_t gbox[2] = {16, 128};
+  const CUresult gr = detail::get_encode_fn()(&gmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, gq.get(), gdims, gstrides, gbox,
+                                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
+                                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  PM_REQUIRE(gr == CUDA_SUCCESS, PACMAP_ERR_CUDA, "cuTensorMapEncodeTiled (column term) failed: " + std::to_string(gr));
 
   DevBuf<uint32_t> cidx(c, n_pad * C);
   DevBuf<float> cv(c, n_pad * C), cu(c, n_pad * C);
@@ -822,7 +874,8 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_CUDA(cudaMemsetAsync(ovf.get() + n, 0, sizeof(uint32_t), c.stream));
   PM_CUDA(cudaMemsetAsync(fbk.get() + n, 0, sizeof(uint32_t), c.stream));
 
-  const size_t smem = 1024 + static_cast<size_t>(2 + TC_STAGES) * KB * KB_BYTES + sizeof(TcShared);
+  const size_t smem =
+      1024 + static_cast<size_t>(2 + TC_STAGES) * KB * KB_BYTES + (TC_STAGES + 1) * G_BYTES + sizeof(TcShared);
   const uint32_t idesc = idesc_f16(bf16);
   const unsigned grid = static_cast<unsigned>(n_pad / TC_BM);
   cudaEvent_t ev[2];
@@ -831,7 +884,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_CUDA(cudaEventRecord(ev[0], c.stream));
   auto launch = [&](auto kern) {
     PM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    kern<<<grid, TC_THREADS, smem, c.stream>>>(map, n, n_pad, idesc, ge.get(), nrm.get(), perm.get(), rank, cidx.get(),
+    kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, idesc, ge.get(), nrm.get(), perm.get(), rank, cidx.get(),
                                              cv.get(), cu.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err);
   };
   if (KB == 1 && PER == 16) launch(knn_filter_kernel<1, 16>);
