@@ -147,21 +147,53 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) gemm_tn_kernel(const __grid_c
           for (int i = 0; i < 16; ++i) v[i] = w[i];
         }
         if (row < o.m_valid) {
+          if (EPI != EPI_F32 && CH == 32 && n0 + c0 + 32 <= o.n_valid && (o.ld_out % 8) == 0 &&
+              (EPI != EPI_DRELU || (o.ld_aux % 8) == 0)) {
+            // 32 bf16 of this row: four 16-byte stores (and four 16-byte loads of the activation)
+            const size_t off = static_cast<size_t>(row) * o.ld_out + n0 + c0;
+            uint4* dst = reinterpret_cast<uint4*>(o.out_bf16 + off);
 #pragma unroll
-          for (int i = 0; i < CH; ++i) {
-            const int col = n0 + c0 + i;
-            if (col >= o.n_valid) continue;
-            float a = v[i];
-            const size_t off = static_cast<size_t>(row) * o.ld_out + col;
-            if (EPI == EPI_F32) {
-              if (o.bias) a += o.bias[col];
-              o.out_f32[off] = a;
-            } else if (EPI == EPI_BIAS_RELU) {
-              a += o.bias[col];
-              o.out_bf16[off] = __float2bfloat16_rn(a > 0.0f ? a : 0.0f);
-            } else {
-              const float h = __bfloat162float(o.aux[static_cast<size_t>(row) * o.ld_aux + col]);
-              o.out_bf16[off] = __float2bfloat16_rn(h > 0.0f ? a : 0.0f);
+            for (int q = 0; q < 4; ++q) {
+              uint32_t w[4];
+              uint4 hv = make_uint4(0u, 0u, 0u, 0u);
+              if (EPI == EPI_DRELU)
+                hv = *reinterpret_cast<const uint4*>(o.aux + static_cast<size_t>(row) * o.ld_aux + n0 + c0 + 8 * q);
+              const uint32_t hw[4] = {hv.x, hv.y, hv.z, hv.w};
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                float lo = v[8 * q + 2 * e], hi = v[8 * q + 2 * e + 1];
+                if (EPI == EPI_BIAS_RELU) {
+                  lo += o.bias[n0 + c0 + 8 * q + 2 * e];
+                  hi += o.bias[n0 + c0 + 8 * q + 2 * e + 1];
+                  lo = lo > 0.0f ? lo : 0.0f;
+                  hi = hi > 0.0f ? hi : 0.0f;
+                } else {
+                  const float hl = __uint_as_float(hw[e] << 16), hh = __uint_as_float(hw[e] & 0xFFFF0000u);
+                  lo = hl > 0.0f ? lo : 0.0f;
+                  hi = hh > 0.0f ? hi : 0.0f;
+                }
+                w[e] = static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(lo))) |
+                       (static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(hi))) << 16);
+              }
+              dst[q] = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < CH; ++i) {
+              const int col = n0 + c0 + i;
+              if (col >= o.n_valid) continue;
+              float a = v[i];
+              const size_t off = static_cast<size_t>(row) * o.ld_out + col;
+              if (EPI == EPI_F32) {
+                if (o.bias) a += o.bias[col];
+                o.out_f32[off] = a;
+              } else if (EPI == EPI_BIAS_RELU) {
+                a += o.bias[col];
+                o.out_bf16[off] = __float2bfloat16_rn(a > 0.0f ? a : 0.0f);
+              } else {
+                const float h = __bfloat162float(o.aux[static_cast<size_t>(row) * o.ld_aux + col]);
+                o.out_bf16[off] = __float2bfloat16_rn(h > 0.0f ? a : 0.0f);
+              }
             }
           }
         }

@@ -3,9 +3,15 @@
 //   x = (x - min); x = x / max           lib.rs:500, 503 (two separately rounded f32 passes)
 //   mean = mean_axis(Axis(0))            lib.rs:506-508 (ndarray: a sequential row-order f32 sum, then / n)
 //   x -= mean                            lib.rs:511
-// The column sum is an inherently serial chain per column; it runs one lane per column with the rows
-// streamed through shared memory by the other warps of the block, so the chain runs at FADD latency.
+// The column sum is an inherently serial chain per column (one rounded f32 add per row, in row
+// order). A parallel pass first writes y = (x - min) / max into a buffer padded to 32 columns; then one
+// warp per 32 columns runs the 32 chains (one lane per column) with the rows streamed into shared
+// memory by a 6-stage TMA pipeline, so each chain runs at FADD latency; the division stays out of the
+// serial warp. The centred output reads the same y.
+#include <cstring>
+
 #include "engine.cuh"
+#include "tcgen05.cuh"
 
 namespace pacmap {
 namespace {
@@ -36,65 +42,151 @@ __global__ void minmax_keys_kernel(const float* __restrict__ x, uint64_t total, 
   }
 }
 
-constexpr int CS_COLS = 8;      // columns per block (one summing lane each)
-constexpr int CS_ROWS = 512;    // rows per staged chunk
-constexpr int CS_THREADS = 256; // warp 0 sums, warps 1..7 stage
+constexpr int CQ_COLS = 32;    // columns per chain warp (one lane each)
+constexpr int CQ_ROWS = 256;   // rows per TMA tile (32 KB)
+constexpr int CQ_STAGES = 6;
 
-__global__ void __launch_bounds__(CS_THREADS) colsum_seq_kernel(const float* __restrict__ x, uint64_t n,
-                                                                uint64_t d, float sub, float div,
-                                                                float* __restrict__ mean) {
-  __shared__ float buf[2][CS_ROWS][CS_COLS];
-  const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * CS_COLS;
-  const int tid = threadIdx.x;
-  const uint64_t nchunks = (n + CS_ROWS - 1) / CS_ROWS;
-  auto stage = [&](uint64_t ch, int slot) {
-    // warps 1..7 load rows [ch*R, ch*R + R) x columns [c0, c0 + 8), applying (v - sub) / div.
-    for (int e = tid - 32; e < CS_ROWS * CS_COLS; e += CS_THREADS - 32) {
-      const int r = e / CS_COLS, cc = e % CS_COLS;
-      const uint64_t row = ch * CS_ROWS + r, col = c0 + cc;
-      float v = 0.0f;
-      if (row < n && col < d) v = __fdiv_rn(__fsub_rn(x[row * d + col], sub), div);
-      buf[slot][r][cc] = v;
-    }
-  };
-  if (tid >= 32) stage(0, 0);
-  __syncthreads();
-  float s = 0.0f;
-  for (uint64_t ch = 0; ch < nchunks; ++ch) {
-    if (tid >= 32 && ch + 1 < nchunks) stage(ch + 1, static_cast<int>((ch + 1) & 1));
-    if (tid < CS_COLS) {
-      const int rows = static_cast<int>((n - ch * CS_ROWS) < CS_ROWS ? (n - ch * CS_ROWS) : CS_ROWS);
-      const int slot = static_cast<int>(ch & 1);
-      int r = 0;
-      for (; r + 16 <= rows; r += 16) {  // loads run ahead of the serial add chain
-        float t[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) t[q] = buf[slot][r + q][tid];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) s = __fadd_rn(s, t[q]);
-      }
-      for (; r < rows; ++r) s = __fadd_rn(s, buf[slot][r][tid]);
-    }
-    __syncthreads();
+// y = (x - sub) / div (two separately rounded f32 operations) into Y [n][dp], padding columns 0.
+__global__ void scale_pad_kernel(const float* __restrict__ x, uint64_t n, uint64_t d, uint64_t dp, float sub,
+                                 float div, float* __restrict__ Y) {
+  const uint64_t total = n * dp;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const uint64_t r = t / dp, c = t - r * dp;
+    Y[t] = c < d ? __fdiv_rn(__fsub_rn(x[r * d + c], sub), div) : 0.0f;
   }
-  if (tid < CS_COLS && c0 + tid < d) mean[c0 + tid] = __fdiv_rn(s, static_cast<float>(n));
 }
 
-__global__ void normalize_center_kernel(const float* __restrict__ x, uint64_t n, uint64_t d, float mn, float mx,
+struct alignas(8) CqShared {
+  uint64_t full[CQ_STAGES];
+  uint64_t empty[CQ_STAGES];
+  int abort_flag;
+};
+
+// mean[c] = (((0 + y_0c) + y_1c) + ... + y_(n-1)c) / n for the 32 columns of this block: warp 1 streams
+// 256-row tiles of Y by TMA, warp 0 runs the chains (the next 16 rows are loaded while the current 16
+// are added). Every wait is bounded.
+__global__ void __launch_bounds__(64) colsum_chain_kernel(const __grid_constant__ CUtensorMap ymap, uint64_t n,
+                                                          uint64_t d, float* __restrict__ mean,
+                                                          uint32_t* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char cq_raw[];
+  float* buf = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(cq_raw) + 127) & ~uintptr_t(127));
+  CqShared* sh = reinterpret_cast<CqShared*>(buf + CQ_STAGES * CQ_ROWS * CQ_COLS);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c0 = blockIdx.x * CQ_COLS;
+  const uint64_t ntiles = (n + CQ_ROWS - 1) / CQ_ROWS;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < CQ_STAGES; ++s) {
+      mbar_init(&sh->full[s], 1);
+      mbar_init(&sh->empty[s], 1);
+    }
+    sh->abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  volatile int* abort_flag = &sh->abort_flag;
+  if (warp == 1) {
+    if (lane == 0) {
+      uint64_t issued = 0;
+      for (uint64_t t = 0; t < ntiles; ++t) {
+        const int s = static_cast<int>(t % CQ_STAGES);
+        if (t >= CQ_STAGES && !mbar_wait(&sh->empty[s], static_cast<uint32_t>(((t / CQ_STAGES) + 1) & 1), abort_flag))
+          break;
+        mbar_expect_tx(&sh->full[s], CQ_ROWS * CQ_COLS * 4);
+        tma_load_2d(buf + s * CQ_ROWS * CQ_COLS, &ymap, &sh->full[s], c0, static_cast<int>(t * CQ_ROWS));
+        issued = t + 1;
+      }
+      if (issued < ntiles) {
+        atomicOr(err, DEV_ERR_TIMEOUT);
+        sh->abort_flag = 1;
+      }
+      // every issued load has landed before the block exits
+      for (uint64_t t = (issued > CQ_STAGES ? issued - CQ_STAGES : 0); t < issued; ++t) {
+        const uint64_t t0 = globaltimer();
+        while (!mbar_try_wait(&sh->full[t % CQ_STAGES], static_cast<uint32_t>((t / CQ_STAGES) & 1)) &&
+               globaltimer() - t0 < WAIT_LIMIT_NS) {
+        }
+      }
+    }
+    return;
+  }
+  float s = 0.0f;
+  for (uint64_t t = 0; t < ntiles; ++t) {
+    const int st = static_cast<int>(t % CQ_STAGES);
+    if (!mbar_wait(&sh->full[st], static_cast<uint32_t>((t / CQ_STAGES) & 1), abort_flag)) {
+      if (lane == 0) {
+        atomicOr(err, DEV_ERR_TIMEOUT);
+        sh->abort_flag = 1;
+      }
+      return;
+    }
+    const float* b = buf + st * CQ_ROWS * CQ_COLS + lane;
+    const int rows = static_cast<int>(n - t * CQ_ROWS < CQ_ROWS ? n - t * CQ_ROWS : CQ_ROWS);
+    int r = 0;
+    if (rows >= 16) {
+      float cur[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) cur[q] = b[q * CQ_COLS];
+      for (r = 16; r + 16 <= rows; r += 16) {
+        float nxt[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) nxt[q] = b[(r + q) * CQ_COLS];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) s = __fadd_rn(s, cur[q]);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) cur[q] = nxt[q];
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) s = __fadd_rn(s, cur[q]);
+    }
+    for (; r < rows; ++r) s = __fadd_rn(s, b[r * CQ_COLS]);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sh->empty[st]);
+  }
+  if (c0 + lane < static_cast<int>(d)) mean[c0 + lane] = __fdiv_rn(s, static_cast<float>(n));
+}
+
+// out = y - mean (lib.rs:511), y read back from the padded buffer.
+__global__ void normalize_center_kernel(const float* __restrict__ Y, uint64_t n, uint64_t d, uint64_t dp,
                                         const float* __restrict__ mean, float* __restrict__ out) {
   const uint64_t total = n * d;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
-    const float y = __fdiv_rn(__fsub_rn(x[t], mn), mx);
-    out[t] = __fsub_rn(y, mean[t % d]);
+    const uint64_t r = t / d, c = t - r * d;
+    out[t] = __fsub_rn(Y[r * dp + c], mean[c]);
   }
 }
 
 }  // namespace
 
-void column_mean_seq(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float sub, float div, float* d_mean) {
-  colsum_seq_kernel<<<ceil_div(d, CS_COLS), CS_THREADS, 0, c.stream>>>(d_x, n, d, sub, div, d_mean);
+// y = (x - sub) / div into Y (pitch dp, returned) and the sequential column means of y.
+uint64_t scaled_column_means(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float sub, float div, DevBuf<float>& Y,
+                             float* d_mean) {
+  const uint64_t dp = (d + CQ_COLS - 1) / CQ_COLS * CQ_COLS;
+  Y.alloc(c, n * dp);
+  const unsigned g = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n * dp, 256), c.sm_count * 16ull));
+  scale_pad_kernel<<<g, 256, 0, c.stream>>>(d_x, n, d, dp, sub, div, Y.get());
   PM_LAUNCHED();
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(dp), static_cast<cuuint64_t>(n)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(dp) * 4};
+  const cuuint32_t box[2] = {CQ_COLS, CQ_ROWS};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult cr = detail::get_encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, Y.get(), dims, strides, box, estr,
+                                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  PM_REQUIRE(cr == CUDA_SUCCESS, PACMAP_ERR_CUDA, "cuTensorMapEncodeTiled (column sums) failed: " + std::to_string(cr));
+  const size_t smem = 128 + static_cast<size_t>(CQ_STAGES) * CQ_ROWS * CQ_COLS * 4 + sizeof(CqShared);
+  PM_CUDA(cudaFuncSetAttribute(colsum_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  colsum_chain_kernel<<<static_cast<unsigned>(dp / CQ_COLS), 64, smem, c.stream>>>(map, n, d, d_mean, c.d_err);
+  PM_LAUNCHED();
+  return dp;
+}
+
+void column_mean_seq(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float sub, float div, float* d_mean) {
+  DevBuf<float> Y;
+  scaled_column_means(c, d_x, n, d, sub, div, Y, d_mean);
 }
 
 void preprocess_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float* d_out, float* h_min, float* h_max,
@@ -125,9 +217,10 @@ void preprocess_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float* 
     mean_local.alloc(c, d);
     mean = mean_local.get();
   }
-  column_mean_seq(c, d_x, n, d, mn, mx, mean);
+  DevBuf<float> Y;
+  const uint64_t dp = scaled_column_means(c, d_x, n, d, mn, mx, Y, mean);
   const unsigned g2 = static_cast<unsigned>(std::min<uint64_t>(ceil_div(total, 256), c.sm_count * 16ull));
-  normalize_center_kernel<<<g2, 256, 0, c.stream>>>(d_x, n, d, mn, mx, mean, d_out);
+  normalize_center_kernel<<<g2, 256, 0, c.stream>>>(Y.get(), n, d, dp, mean, d_out);
   PM_LAUNCHED();
 }
 
