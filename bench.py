@@ -235,13 +235,16 @@ def run_ours(args, rank, world, local_rank):
             tdist.barrier()
         torch.cuda.synchronize()
 
+    # every library call enqueues its kernels on the library's own stream: time on that stream
+    lib_stream = torch.cuda.ExternalStream(_abi.lib().pacmap_device_stream(local_rank), device=dev)
+
     def timed(fn, k):
         barrier()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record()
+        ev0.record(lib_stream)
         for _ in range(k):
             fn()
-        ev1.record()
+        ev1.record(lib_stream)
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1)
         barrier()

@@ -234,6 +234,9 @@ pacmap_status pacmap_preprocess_noalloc(const float* d_x, uint64_t n, uint64_t d
 void pacmap_set_stage_timing(int32_t enabled);
 uint64_t pacmap_stage_times(double* out_ms, uint64_t cap);
 
+/* The CUDA stream (cudaStream_t) on which every call for `device` enqueues its work, so that a caller
+ * can time calls with events on the launching stream (no reference analogue); NULL on error. */
+void* pacmap_device_stream(int32_t device);
 /* Kernel launches issued by this thread since the last call of this function (diagnostics). */
 uint64_t pacmap_take_launch_count(void);
 

@@ -338,6 +338,16 @@ uint64_t pacmap_stage_times(double* out_ms, uint64_t cap) {
   return g_stage_ms.size();
 }
 
+void* pacmap_device_stream(int32_t device) {
+  try {
+    DeviceLock dl(device);
+    return static_cast<void*>(dl.ctx.stream);
+  } catch (const Fail& f) {
+    set_last_error(f.msg);
+    return nullptr;
+  }
+}
+
 uint64_t pacmap_take_launch_count(void) {
   const uint64_t v = g_launches;
   g_launches = 0;

@@ -611,7 +611,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const float e4_i = valid ? ge[row].y : 0.0f;
     const uint64_t cbase = row * static_cast<uint64_t>(C);
     bool ok = true;
-    auto screen = [&](const uint32_t (&r)[32], int colb) {
+    // e4v: this lane's 4 e_j for column colb + lane; an insertion at column c takes lane c's value.
+    auto screen = [&](const uint32_t (&r)[32], int colb, float e4v) {
       float m8[4];
 #pragma unroll
       for (int g = 0; g < 4; ++g) {
@@ -625,12 +626,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
           if (__any_sync(0xFFFFFFFFu, -2.0f * m8[g] <= theta)) {
 #pragma unroll
             for (int c = 8 * g; c < 8 * g + 8; ++c) {
+              const float e4j = __shfl_sync(0xFFFFFFFFu, e4v, c);
               const float v = -2.0f * __uint_as_float(r[c]);
               if (v <= theta) {
-                const int col = colb + c;
-                cand_idx[cbase + cnt] = static_cast<uint32_t>(col);
+                cand_idx[cbase + cnt] = static_cast<uint32_t>(colb + c);
                 cand_v[cbase + cnt] = v;
-                cand_u[cbase + cnt] = v + __ldg(&ge[col].y);
+                cand_u[cbase + cnt] = v + e4j;
                 ++cnt;
               }
             }
@@ -638,8 +639,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         }
       }
     };
+    // The 4 e_j of each tile are loaded one tile ahead (coalesced), so an insertion never waits on memory.
+    float e4n[4];
+    {
+      const int c0n = sweep_tile(0, static_cast<int>(blockIdx.x), ntiles) * TC_BN;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) e4n[q] = __ldg(&ge[c0n + 32 * q + lane].y);
+    }
     for (int t = 0; t < ntiles; ++t) {
       const int acc = t & 1;
+      float e4c[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) e4c[q] = e4n[q];
+      if (t + 1 < ntiles) {
+        const int c0n = sweep_tile(t + 1, static_cast<int>(blockIdx.x), ntiles) * TC_BN;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e4n[q] = __ldg(&ge[c0n + 32 * q + lane].y);
+      }
       if (!mbar_wait(&sh->tmem_full[acc], (t >> 1) & 1, abort_flag)) {
         ok = false;
         break;
@@ -647,15 +663,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
       tc_fence_after();
       const int col0 = sweep_tile(t, static_cast<int>(blockIdx.x), ntiles) * TC_BN;
       const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) + acc * 256 + half * 128;
-#pragma unroll 1
+#pragma unroll
       for (int cp = 0; cp < 2; ++cp) {  // 64 columns per pass, two TMEM loads in flight
         uint32_t r0[32], r1[32];
         tmem_ld32_issue(taddr + cp * 64, r0);
         tmem_ld32_issue(taddr + cp * 64 + 32, r1);
         tmem_wait_ld_tied(r0);
         tie_regs(r1);
-        screen(r0, col0 + cp * 64);
-        screen(r1, col0 + cp * 64 + 32);
+        screen(r0, col0 + cp * 64, e4c[2 * cp]);
+        screen(r1, col0 + cp * 64 + 32, e4c[2 * cp + 1]);
       }
       tc_fence_before();
       __syncwarp();

@@ -70,6 +70,7 @@ _SIGS = {
     "pacmap_mlp_grad": (C.c_int, [_vp, _u64, _u64, _vp, _vp, _u64, _i32, _vp, _vp]),
     "pacmap_fit_transform_learned": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp, _vp]),
     "pacmap_fit_transform_learned_device": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp, _vp]),
+    "pacmap_device_stream": (C.c_void_p, [_i32]),
     "pacmap_take_launch_count": (C.c_uint64, []),
     "pacmap_set_stage_timing": (None, [_i32]),
     "pacmap_stage_times": (C.c_uint64, [_vp, _u64]),
