@@ -278,33 +278,25 @@ __device__ __forceinline__ void load_y(const float* __restrict__ y, uint32_t j, 
   }
 }
 
-template <int DIM>
-__device__ __forceinline__ void accumulate_row(const float* __restrict__ y, const uint32_t* __restrict__ col,
-                                               uint32_t s0, uint32_t s1, uint32_t s2, uint32_t s3, bool use_mn,
-                                               int gl, int G, const float (&yi)[DIM], const Sched& sc,
-                                               float (&acc)[DIM], float& lacc, bool want_loss) {
-  const uint32_t nnn = s1 - s0, nmn = use_mn ? (s2 - s1) : 0u;
-  const uint32_t total = nnn + nmn + (s3 - s2);
-  auto where = [&](uint32_t q) -> uint32_t {
-    return q < nnn ? s0 + q : (q < nnn + nmn ? s1 + (q - nnn) : s2 + (q - nnn - nmn));
-  };
-  uint32_t q = static_cast<uint32_t>(gl);
-  if (q >= total) return;
-  uint32_t ja = col[where(q)];
-  const uint32_t qb0 = q + G;
-  uint32_t jb = qb0 < total ? col[where(qb0)] : 0u;
+// One segment (one pair type) of a row: lane gl of a G-lane group takes entries s + gl, s + gl + G, ...
+// in that order, with the partner index and y of the next entry loaded ahead (two-deep pipeline).
+// The type's constants (c1, c2, weight, sign) are fixed for the whole segment.
+template <int DIM, bool REPULSIVE>
+__device__ __forceinline__ void accumulate_segment(const float* __restrict__ y, const uint32_t* __restrict__ col,
+                                                   uint32_t s, uint32_t e, int gl, int G, const float (&yi)[DIM],
+                                                   float c1, float c2, float w, float (&acc)[DIM], float& lacc,
+                                                   bool want_loss) {
+  uint32_t j = s + static_cast<uint32_t>(gl);
+  if (j >= e) return;
+  const uint32_t g = static_cast<uint32_t>(G);
+  uint32_t ja = col[j];
+  uint32_t jb = j + g < e ? col[j + g] : 0u;
   float ya[DIM];
   load_y<DIM>(y, ja, ya);
-  for (; q < total; q += G) {
-    const uint32_t qb = q + G, qc = q + 2 * G;
+  for (; j < e; j += g) {
     float yb[DIM];
-    if (qb < total) load_y<DIM>(y, jb, yb);
-    const uint32_t jc = qc < total ? col[where(qc)] : 0u;
-    const int ty = q < nnn ? 0 : (q < nnn + nmn ? 1 : 2);
-    const bool fp = ty == 2;
-    const float c1 = ty == 0 ? 10.0f : (ty == 1 ? 10000.0f : 1.0f);
-    const float c2 = ty == 0 ? 20.0f : (ty == 1 ? 20000.0f : 2.0f);
-    const float w = ty == 0 ? sc.w_nn : (ty == 1 ? sc.w_mn : sc.w_fp);
+    if (j + g < e) load_y<DIM>(y, jb, yb);
+    const uint32_t jc = j + 2 * g < e ? col[j + 2 * g] : 0u;
     float df[DIM];
     float dsq = 1.0f;
 #pragma unroll
@@ -317,14 +309,27 @@ __device__ __forceinline__ void accumulate_row(const float* __restrict__ y, cons
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
       const float gterm = __fmul_rn(w1, df[c]);
-      acc[c] = __fadd_rn(acc[c], fp ? -gterm : gterm);
+      acc[c] = __fadd_rn(acc[c], REPULSIVE ? -gterm : gterm);
     }
     if (want_loss)
-      lacc += fp ? __fmul_rn(w, __fdiv_rn(1.0f, __fadd_rn(1.0f, dsq))) : __fmul_rn(w, __fdiv_rn(dsq, tt));
+      lacc += REPULSIVE ? __fmul_rn(w, __fdiv_rn(1.0f, __fadd_rn(1.0f, dsq))) : __fmul_rn(w, __fdiv_rn(dsq, tt));
 #pragma unroll
     for (int c = 0; c < DIM; ++c) ya[c] = yb[c];
     jb = jc;
   }
+}
+
+// A row's forces: the NN, MN (skipped when w_mn = 0) and FP segments in turn (per-pair arithmetic of
+// gradient.rs:120-147: c = 10, 10000 and 1 in the denominators, FP repulsive).
+template <int DIM>
+__device__ __forceinline__ void accumulate_row(const float* __restrict__ y, const uint32_t* __restrict__ col,
+                                               uint32_t s0, uint32_t s1, uint32_t s2, uint32_t s3, bool use_mn,
+                                               int gl, int G, const float (&yi)[DIM], const Sched& sc,
+                                               float (&acc)[DIM], float& lacc, bool want_loss) {
+  accumulate_segment<DIM, false>(y, col, s0, s1, gl, G, yi, 10.0f, 20.0f, sc.w_nn, acc, lacc, want_loss);
+  if (use_mn)
+    accumulate_segment<DIM, false>(y, col, s1, s2, gl, G, yi, 10000.0f, 20000.0f, sc.w_mn, acc, lacc, want_loss);
+  accumulate_segment<DIM, true>(y, col, s2, s3, gl, G, yi, 1.0f, 2.0f, sc.w_fp, acc, lacc, want_loss);
 }
 
 template <int G, int DIM>
