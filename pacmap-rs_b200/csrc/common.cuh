@@ -169,6 +169,43 @@ struct PointStream {
   }
 };
 
+// The same word sequence as PointStream, produced by a whole warp: lane L computes block base + L, so
+// one Philox call per lane serves 128 draws, and word w of the batch comes from lane w / 4 by shuffle.
+// Every lane must call next() / uniform() together (warp-uniform control flow).
+struct WarpStream {
+  uint32_t k0, k1, c1, c2, base;
+  uint32_t buf[4];
+  int pos;
+  __device__ __forceinline__ WarpStream(uint64_t seed, uint64_t point)
+      : k0(static_cast<uint32_t>(seed)), k1(static_cast<uint32_t>(seed >> 32)),
+        c1(static_cast<uint32_t>(point)), c2(static_cast<uint32_t>(point >> 32)), base(0), pos(128) {}
+  __device__ __forceinline__ uint32_t next() {
+    if (pos == 128) {
+      philox4x32_10(base + (threadIdx.x & 31u), c1, c2, TAG_SAMPLE, k0, k1, buf);
+      base += 32;
+      pos = 0;
+    }
+    const int t = pos & 3;
+    const uint32_t mine = t == 0 ? buf[0] : (t == 1 ? buf[1] : (t == 2 ? buf[2] : buf[3]));
+    const uint32_t w = __shfl_sync(0xFFFFFFFFu, mine, pos >> 2);
+    ++pos;
+    return w;
+  }
+  __device__ __forceinline__ bool uniform(uint32_t range, uint32_t& out, uint64_t& budget) {
+    const uint32_t zone = (range << __clz(range)) - 1u;
+    while (budget > 0) {
+      --budget;
+      const uint32_t w = next();
+      const uint32_t lo = w * range;
+      if (lo <= zone) {
+        out = __umulhi(w, range);
+        return true;
+      }
+    }
+    return false;
+  }
+};
+
 constexpr uint64_t SAMPLE_ATTEMPT_CAP = 1ull << 26;
 
 // ---------------------------------------------------------------------------------------------

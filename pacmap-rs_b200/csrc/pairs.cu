@@ -9,8 +9,12 @@
 //   K6 sample_mn_kernel: mid-near pairs (sampling.rs:118-142, 296-313): per slot, 6 distinct
 //      candidates (not the point, not an earlier pick), the 2nd smallest reference f32 distance wins.
 //
-// Both samplers give one warp to one point: every lane replays the same Philox stream (no shuffles
-// for the draws), membership tests are split across lanes and combined with a ballot.
+// Both samplers give one warp to one point. The fast variants draw from a WarpStream (each lane
+// computes one Philox block per 128 words and the words are shuffled out) and keep the point's
+// exclusion lists in registers (slot s in lane s % 32, register s / 32), so a membership test is one
+// compare per register and a vote; the MN variant also keeps row i of x in registers. The general
+// variants (every lane replays the stream, lists read from memory) serve the shapes beyond those
+// registers. Both variants consume the same words in the same order: the pairs are identical.
 #include "engine.cuh"
 
 namespace pacmap {
@@ -98,6 +102,64 @@ __global__ void sample_fp_kernel(const uint32_t* __restrict__ pnn, uint64_t n, u
         out[(i * n_fp + cnt) * 2 + 1] = j;
       }
       __syncwarp();
+      ++cnt;
+    }
+  }
+}
+
+// True when any lane holds v in one of its R registers of a lane-distributed list of `len` slots.
+template <int R>
+__device__ __forceinline__ bool reg_contains(const uint32_t (&reg)[R], uint32_t len, uint32_t v) {
+  const uint32_t lane = lane_id();
+  bool hit = false;
+#pragma unroll
+  for (int r = 0; r < R; ++r) hit |= (lane + 32u * r < len) && reg[r] == v;
+  return __any_sync(0xFFFFFFFFu, hit);
+}
+template <int R>
+__device__ __forceinline__ void reg_put(uint32_t (&reg)[R], uint32_t slot, uint32_t v) {
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    if (lane + 32u * r == slot) reg[r] = v;
+}
+
+// sample_fp_kernel with the picks (n_fp <= 32 PR) and the k neighbours (k <= 32 RR) in registers.
+template <int PR, int RR>
+__global__ void sample_fp_reg_kernel(const uint32_t* __restrict__ pnn, uint64_t n, uint32_t k, uint32_t n_fp,
+                                     uint64_t seed, uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  const uint32_t lane = lane_id();
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    uint32_t rej[RR], pk[PR];
+#pragma unroll
+    for (int r = 0; r < RR; ++r) {
+      const uint32_t t = lane + 32u * r;
+      rej[r] = t < k ? pnn[((i * k) + t) * 2 + 1] : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < PR; ++r) pk[r] = 0u;
+    const bool self_in = reg_contains<RR>(rej, k, static_cast<uint32_t>(i));
+    uint64_t avail = n > k ? n - k : 0;
+    const uint64_t self_cut = self_in ? 0 : 1;
+    avail = avail > self_cut ? avail - self_cut : 0;
+    const uint32_t want = static_cast<uint32_t>((n_fp < avail ? static_cast<uint64_t>(n_fp) : avail));
+    WarpStream s(seed, i);
+    uint64_t budget = SAMPLE_ATTEMPT_CAP;
+    uint32_t cnt = 0;
+    while (cnt < want) {
+      uint32_t j;
+      if (!s.uniform(static_cast<uint32_t>(n), j, budget)) {
+        if (lane == 0) atomicOr(err, DEV_ERR_SAMPLING);
+        break;
+      }
+      if (j == i) continue;
+      if (reg_contains<PR>(pk, cnt, j) || reg_contains<RR>(rej, k, j)) continue;
+      reg_put<PR>(pk, cnt, j);
+      if (lane == (cnt & 31u)) {
+        out[(i * n_fp + cnt) * 2 + 0] = static_cast<uint32_t>(i);
+        out[(i * n_fp + cnt) * 2 + 1] = j;
+      }
       ++cnt;
     }
   }
@@ -212,6 +274,116 @@ __global__ void sample_mn_kernel(const float* __restrict__ x, uint64_t n, int d,
   }
 }
 
+// sample_mn_kernel with the picks (n_mn <= 32) in one register per lane and row i of x (d <= 8 NC)
+// in NC registers of each 8-lane group.
+template <int NC>
+__global__ void sample_mn_reg_kernel(const float* __restrict__ x, uint64_t n, int d, uint32_t n_mn, uint64_t seed,
+                                     uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  const uint32_t lane = lane_id();
+  const int l8 = lane & 7;
+  const unsigned gbase = lane & ~7u;
+  const int grp = lane >> 3;
+  const int nc = d >> 3;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const float* a = x + i * d;
+    float ra[NC];
+#pragma unroll
+    for (int ch = 0; ch < NC; ++ch) ra[ch] = ch < nc ? a[8 * ch + l8] : 0.0f;
+    uint32_t pk[1] = {0u};
+    WarpStream s(seed, i);
+    uint64_t budget = SAMPLE_ATTEMPT_CAP;
+    bool failed = false;
+    for (uint32_t jslot = 0; jslot < n_mn && !failed; ++jslot) {
+      const bool self_in = reg_contains<1>(pk, jslot, static_cast<uint32_t>(i));
+      uint64_t avail = n > jslot ? n - jslot : 0;
+      const uint64_t self_cut = self_in ? 0 : 1;
+      avail = avail > self_cut ? avail - self_cut : 0;
+      const uint32_t want = static_cast<uint32_t>((avail < 6 ? avail : 6ull));
+      uint32_t cand[6] = {0, 0, 0, 0, 0, 0};
+      uint32_t cnt = 0;
+      while (cnt < want) {
+        uint32_t j;
+        if (!s.uniform(static_cast<uint32_t>(n), j, budget)) {
+          failed = true;
+          break;
+        }
+        if (j == i) continue;
+        bool dup = false;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) dup |= (t < static_cast<int>(cnt) && cand[t] == j);
+        if (dup || reg_contains<1>(pk, jslot, j)) continue;
+#pragma unroll
+        for (int t = 0; t < 6; ++t)
+          if (t == static_cast<int>(cnt)) cand[t] = j;
+        ++cnt;
+      }
+      if (failed) {
+        if (lane == 0) atomicOr(err, DEV_ERR_SAMPLING);
+        break;
+      }
+      // Distances of the drawn candidates in the reference's order (group8_ref_dist with row i in
+      // registers): group g (lanes 8g..8g+7) handles slots g and g + 4.
+      float dist[6];
+#pragma unroll
+      for (int pass = 0; pass < 2; ++pass) {
+        const int slot = pass * 4 + grp;
+        uint32_t cidx = 0;
+#pragma unroll
+        for (int t = 0; t < 6; ++t)
+          if (t == slot) cidx = cand[t];
+        const bool active = slot < static_cast<int>(cnt);
+        const float* b = x + static_cast<uint64_t>(active ? cidx : i) * d;
+        float acc = 0.0f;
+#pragma unroll
+        for (int ch = 0; ch < NC; ++ch) {
+          if (ch < nc) {
+            const float df = __fsub_rn(ra[ch], b[8 * ch + l8]);
+            acc = __fadd_rn(acc, __fmul_rn(df, df));
+          }
+        }
+        float tsum = 0.0f;
+#pragma unroll
+        for (int l = 0; l < 8; ++l) tsum = __fadd_rn(tsum, __shfl_sync(0xFFFFFFFFu, acc, gbase + l));
+        for (int e = nc * 8; e < d; ++e) {
+          const float df = __fsub_rn(a[e], b[e]);
+          tsum = __fadd_rn(tsum, __fmul_rn(df, df));
+        }
+        const float dv = active ? __fsqrt_rn(tsum) : 0.0f;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const float vv = __shfl_sync(0xFFFFFFFFu, dv, g * 8);
+          if (pass * 4 + g < 6) dist[pass * 4 + g] = vv;
+        }
+      }
+      // Slots >= cnt are the reference's (0.0, 0) fill. Pick the 2nd smallest (key, slot).
+      uint64_t best0 = ~0ull, best1 = ~0ull;
+      uint32_t id0 = 0, id1 = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const bool real = t < static_cast<int>(cnt);
+        const float dv = real ? dist[t] : 0.0f;
+        const uint32_t id = real ? cand[t] : 0u;
+        const uint64_t key = (static_cast<uint64_t>(total_key(dv)) << 3) | static_cast<uint64_t>(t);
+        if (key < best0) {
+          best1 = best0;
+          id1 = id0;
+          best0 = key;
+          id0 = id;
+        } else if (key < best1) {
+          best1 = key;
+          id1 = id;
+        }
+      }
+      reg_put<1>(pk, jslot, id1);
+      if (lane == 0) {
+        out[(i * n_mn + jslot) * 2 + 0] = static_cast<uint32_t>(i);
+        out[(i * n_mn + jslot) * 2 + 1] = id1;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 void sigma_device(Ctx& c, const float* d_kd, uint64_t n, uint64_t kp, float* d_sig) {
@@ -238,8 +410,13 @@ void sample_fp_device(Ctx& c, const uint32_t* d_pnn, uint64_t n, uint64_t k, uin
   PM_REQUIRE(n < (1ull << 32), PACMAP_ERR_UNSUPPORTED, "pair indices are u32: n must be < 2^32");
   PM_CUDA(cudaMemsetAsync(d_pfp, 0, n * n_fp * 2 * sizeof(uint32_t), c.stream));
   const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n, 8), c.sm_count * 32ull));
-  sample_fp_kernel<<<grid, 256, 0, c.stream>>>(d_pnn, n, static_cast<uint32_t>(k), static_cast<uint32_t>(n_fp), seed,
-                                               d_pfp, c.d_err);
+  const uint32_t k32 = static_cast<uint32_t>(k), f32n = static_cast<uint32_t>(n_fp);
+  if (n_fp <= 96 && k <= 64)
+    sample_fp_reg_kernel<3, 2><<<grid, 256, 0, c.stream>>>(d_pnn, n, k32, f32n, seed, d_pfp, c.d_err);
+  else if (n_fp <= 256 && k <= 128)
+    sample_fp_reg_kernel<8, 4><<<grid, 256, 0, c.stream>>>(d_pnn, n, k32, f32n, seed, d_pfp, c.d_err);
+  else
+    sample_fp_kernel<<<grid, 256, 0, c.stream>>>(d_pnn, n, k32, f32n, seed, d_pfp, c.d_err);
   PM_LAUNCHED();
 }
 
@@ -249,8 +426,14 @@ void sample_mn_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, uint64_
   PM_REQUIRE(n < (1ull << 32), PACMAP_ERR_UNSUPPORTED, "pair indices are u32: n must be < 2^32");
   PM_CUDA(cudaMemsetAsync(d_pmn, 0, n * n_mn * 2 * sizeof(uint32_t), c.stream));
   const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n, 8), c.sm_count * 32ull));
-  sample_mn_kernel<<<grid, 256, 0, c.stream>>>(d_xp, n, static_cast<int>(d), static_cast<uint32_t>(n_mn), seed,
-                                               d_pmn, c.d_err);
+  const int di = static_cast<int>(d);
+  const uint32_t m32 = static_cast<uint32_t>(n_mn);
+  if (n_mn <= 32 && d <= 128)
+    sample_mn_reg_kernel<16><<<grid, 256, 0, c.stream>>>(d_xp, n, di, m32, seed, d_pmn, c.d_err);
+  else if (n_mn <= 32 && d <= 256)
+    sample_mn_reg_kernel<32><<<grid, 256, 0, c.stream>>>(d_xp, n, di, m32, seed, d_pmn, c.d_err);
+  else
+    sample_mn_kernel<<<grid, 256, 0, c.stream>>>(d_xp, n, di, m32, seed, d_pmn, c.d_err);
   PM_LAUNCHED();
 }
 
