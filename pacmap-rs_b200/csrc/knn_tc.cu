@@ -480,7 +480,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
   // 1024-byte aligned operand region: A [2 halves][KB][16 KB], the all-ones tile [4 KB], the
   // column-term tiles [STAGES][4 KB], B [STAGES][KB][16 KB], then TcShared (the small tiles sit below
   // the large B stages).
-  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
+  // aligned by offsetting the shared array itself, so every access keeps the shared address space
+  unsigned char* base = tc_smem_raw + ((1024u - (smem_u32(tc_smem_raw) & 1023u)) & 1023u);
   unsigned char* a_smem = base;
   unsigned char* one_smem = base + 2 * KB * KB_BYTES;
   unsigned char* g_smem = one_smem + G_BYTES;

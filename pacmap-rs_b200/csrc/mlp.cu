@@ -58,7 +58,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) gemm_tn_kernel(const __grid_c
                                                                   GemmOut o, uint32_t* __restrict__ err) {
   constexpr int B_STAGE = BN * 128;
   extern __shared__ __align__(1024) unsigned char gemm_raw[];
-  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(gemm_raw) + 1023) & ~uintptr_t(1023));
+  // aligned by offsetting the shared array itself, so every access keeps the shared address space
+  unsigned char* base = gemm_raw + ((1024u - (smem_u32(gemm_raw) & 1023u)) & 1023u);
   unsigned char* a_s = base;
   unsigned char* b_s = base + GEMM_STAGES * A_STAGE;
   GemmShared* sh = reinterpret_cast<GemmShared*>(b_s + GEMM_STAGES * B_STAGE);

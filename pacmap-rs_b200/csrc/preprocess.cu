@@ -70,7 +70,8 @@ __global__ void __launch_bounds__(64) colsum_chain_kernel(const __grid_constant_
                                                           uint64_t d, float* __restrict__ mean,
                                                           uint32_t* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char cq_raw[];
-  float* buf = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(cq_raw) + 127) & ~uintptr_t(127));
+  // aligned by offsetting the shared array itself: the chain's loads stay shared-memory loads
+  float* buf = reinterpret_cast<float*>(cq_raw + ((128u - (smem_u32(cq_raw) & 127u)) & 127u));
   CqShared* sh = reinterpret_cast<CqShared*>(buf + CQ_STAGES * CQ_ROWS * CQ_COLS);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c0 = blockIdx.x * CQ_COLS;
