@@ -717,46 +717,67 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
 // ---------------------------------------------------------------------------------------------
 // 3. exact re-rank: one warp per (permuted) row; output at the original row, original indices.
 // ---------------------------------------------------------------------------------------------
-constexpr int RR_WARPS = 4;
+// 3a. final compaction: the row's certified band (v <= theta of its rank-th upper bound), one warp
+//     per row; the count is written back (rows that overflowed in the filter keep -1).
+constexpr int RC_WARPS = 4;
 
 template <int PER>
-__global__ void __launch_bounds__(RR_WARPS * 32) knn_rerank_kernel(
-    const float* __restrict__ x, uint64_t n, int d, int K, int rank, const float* __restrict__ nrm,
-    const float2* __restrict__ ge, const uint32_t* __restrict__ perm, uint32_t* __restrict__ cand_idx,
-    float* __restrict__ cand_v, float* __restrict__ cand_u, const int* __restrict__ cand_cnt,
-    uint32_t* __restrict__ out_idx, float* __restrict__ out_dist, uint32_t* __restrict__ fallback_rows,
-    uint32_t* __restrict__ n_fallback) {
+__global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
+    uint64_t n, int rank, const float* __restrict__ nrm, const float2* __restrict__ ge, uint32_t* __restrict__ cand_idx,
+    float* __restrict__ cand_v, float* __restrict__ cand_u, int* __restrict__ cand_cnt) {
   constexpr int C = 32 * PER;
-  __shared__ uint64_t keys_all[RR_WARPS][C];
-  __shared__ uint32_t hist_all[RR_WARPS][256];
+  __shared__ uint32_t hist_all[RC_WARPS][256];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* hist = hist_all[warp];
+  for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * RC_WARPS + warp; r < n;
+       r += static_cast<uint64_t>(gridDim.x) * RC_WARPS) {
+    const int m0 = min(cand_cnt[r], C);
+    if (m0 <= 0) continue;
+    const uint64_t rb = r * static_cast<uint64_t>(C);
+    float th;
+    const int m = warp_compact_regs<PER>(cand_idx + rb, cand_v + rb, cand_u + rb, m0, min(rank, m0), nrm[r], ge[r].y,
+                                         hist, th);
+    if (lane == 0) cand_cnt[r] = m;
+  }
+}
+
+// 3b. exact re-rank of the compacted band: the reference's f32 distance of every survivor (8-lane
+//     groups in distance.rs:50-75's lane order, 4 survivors per warp pass, row i of x in registers),
+//     sorted by (distance, index); output at the original row, original indices.
+template <int PER, int WARPS, int NC>
+__global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
+    const float* __restrict__ x, uint64_t n, int d, int K, const uint32_t* __restrict__ perm,
+    const uint32_t* __restrict__ cand_idx, const int* __restrict__ cand_cnt, uint32_t* __restrict__ out_idx,
+    float* __restrict__ out_dist, uint32_t* __restrict__ fallback_rows, uint32_t* __restrict__ n_fallback) {
+  constexpr int C = 32 * PER;
+  __shared__ uint64_t keys_all[WARPS][C];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint64_t* keys = keys_all[warp];
-  uint32_t* hist = hist_all[warp];
   const int l8 = lane & 7, grp = lane >> 3;
-  for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * RR_WARPS + warp; r < n;
-       r += static_cast<uint64_t>(gridDim.x) * RR_WARPS) {
-    const int m0 = min(cand_cnt[r], C);
-    if (m0 < 0) continue;  // overflowed in the filter: handled by the exact fallback
+  const int nc = d >> 3;
+  for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * WARPS + warp; r < n;
+       r += static_cast<uint64_t>(gridDim.x) * WARPS) {
+    const int m = min(cand_cnt[r], C);
+    if (m < 0) continue;  // overflowed in the filter: handled by the exact fallback
     const uint64_t rb = r * static_cast<uint64_t>(C);
     const uint64_t orow = perm[r];
-    int m = m0;
-    if (m > 0) {
-      float th;
-      m = warp_compact_regs<PER>(cand_idx + rb, cand_v + rb, cand_u + rb, m, min(rank, m), nrm[r], ge[r].y, hist, th);
-    }
-    // exact reference distances of the survivors (self excluded), 4 at a time per warp
-    int nk = 0;
     const float* a = x + orow * d;
+    float ra[NC];
+#pragma unroll
+    for (int ch = 0; ch < NC; ++ch) ra[ch] = ch < nc ? a[8 * ch + l8] : 0.0f;
+    int nk = 0;
     for (int e0 = 0; e0 < m; e0 += 4) {
       const int e = e0 + grp;
       const uint32_t jp = (e < m) ? cand_idx[rb + e] : static_cast<uint32_t>(r);
       const uint32_t j = perm[jp];
       const float* b = x + static_cast<uint64_t>(j) * d;
       float accl = 0.0f;
-      const int nc = d >> 3;
-      for (int ch = 0; ch < nc; ++ch) {
-        const float df = __fsub_rn(a[8 * ch + l8], b[8 * ch + l8]);
-        accl = __fadd_rn(accl, __fmul_rn(df, df));
+#pragma unroll
+      for (int ch = 0; ch < NC; ++ch) {
+        if (ch < nc) {
+          const float df = __fsub_rn(ra[ch], b[8 * ch + l8]);
+          accl = __fadd_rn(accl, __fmul_rn(df, df));
+        }
       }
       float t = 0.0f;
 #pragma unroll
@@ -917,15 +938,32 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   cudaEventDestroy(ev[1]);
   last_tc_filter_ms() = fms;
 
-  const unsigned rgrid = std::min<unsigned>(ceil_div(n, RR_WARPS), c.sm_count * 16);
+  const unsigned cgrid = std::min<unsigned>(ceil_div(n, RC_WARPS), c.sm_count * 16);
   if (PER == 16)
-    knn_rerank_kernel<16><<<rgrid, RR_WARPS * 32, 0, c.stream>>>(d_x, n, static_cast<int>(d), static_cast<int>(kp), rank,
-                                                               nrm.get(), ge.get(), perm.get(), cidx.get(), cv.get(),
-                                                               cu.get(), ccnt.get(), d_idx, d_dist, fbk.get(), fbk.get() + n);
+    knn_compact_kernel<16><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cidx.get(), cv.get(),
+                                                                  cu.get(), ccnt.get());
   else
-    knn_rerank_kernel<32><<<rgrid, RR_WARPS * 32, 0, c.stream>>>(d_x, n, static_cast<int>(d), static_cast<int>(kp), rank,
-                                                               nrm.get(), ge.get(), perm.get(), cidx.get(), cv.get(),
-                                                               cu.get(), ccnt.get(), d_idx, d_dist, fbk.get(), fbk.get() + n);
+    knn_compact_kernel<32><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cidx.get(), cv.get(),
+                                                                  cu.get(), ccnt.get());
+  PM_LAUNCHED();
+  const int di = static_cast<int>(d), ki = static_cast<int>(kp);
+  if (PER == 16) {
+    const unsigned rgrid = std::min<unsigned>(ceil_div(n, 8), c.sm_count * 32);
+    if (d > 64)
+      knn_rerank_kernel<16, 8, 16><<<rgrid, 256, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cidx.get(), ccnt.get(), d_idx,
+                                                                d_dist, fbk.get(), fbk.get() + n);
+    else
+      knn_rerank_kernel<16, 8, 8><<<rgrid, 256, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cidx.get(), ccnt.get(), d_idx,
+                                                               d_dist, fbk.get(), fbk.get() + n);
+  } else {
+    const unsigned rgrid = std::min<unsigned>(ceil_div(n, 4), c.sm_count * 32);
+    if (d > 64)
+      knn_rerank_kernel<32, 4, 16><<<rgrid, 128, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cidx.get(), ccnt.get(), d_idx,
+                                                                d_dist, fbk.get(), fbk.get() + n);
+    else
+      knn_rerank_kernel<32, 4, 8><<<rgrid, 128, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cidx.get(), ccnt.get(), d_idx,
+                                                               d_dist, fbk.get(), fbk.get() + n);
+  }
   PM_LAUNCHED();
 
   // Rows the filter could not settle: exact SIMT recomputation, scattered into place.
