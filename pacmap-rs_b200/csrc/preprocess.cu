@@ -147,9 +147,10 @@ __global__ void __launch_bounds__(64) colsum_chain_kernel(const __grid_constant_
   if (c0 + lane < static_cast<int>(d)) mean[c0 + lane] = __fdiv_rn(s, static_cast<float>(n));
 }
 
-// out = y - mean (lib.rs:511), y read back from the padded buffer.
-__global__ void normalize_center_kernel(const float* __restrict__ Y, uint64_t n, uint64_t d, uint64_t dp,
-                                        const float* __restrict__ mean, float* __restrict__ out) {
+// out = y - mean (lib.rs:511); y may be `out` itself (same pitch), each element read then written by
+// one thread.
+__global__ void normalize_center_kernel(const float* Y, uint64_t n, uint64_t d, uint64_t dp,
+                                        const float* __restrict__ mean, float* out) {
   const uint64_t total = n * d;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
@@ -160,13 +161,19 @@ __global__ void normalize_center_kernel(const float* __restrict__ Y, uint64_t n,
 
 }  // namespace
 
-// y = (x - sub) / div into Y (pitch dp, returned) and the sequential column means of y.
-uint64_t scaled_column_means(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float sub, float div, DevBuf<float>& Y,
-                             float* d_mean) {
-  const uint64_t dp = (d + CQ_COLS - 1) / CQ_COLS * CQ_COLS;
-  Y.alloc(c, n * dp);
+// y = (x - sub) / div with pitch dp = d rounded up to 4 floats (the TMA stride rule), written into
+// `dst` when that pitch is d and dst is 16-byte aligned (no scratch at all), else into Y; then the
+// sequential column means of y (the 32-column TMA boxes zero-fill columns beyond dp). Returns y.
+const float* scaled_column_means(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float sub, float div, float* dst,
+                                 DevBuf<float>& Y, float* d_mean, uint64_t& dp_out) {
+  const uint64_t dp = (d + 3) / 4 * 4;
+  float* y = dst;
+  if (!(dst && dp == d && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0)) {
+    Y.alloc(c, n * dp);
+    y = Y.get();
+  }
   const unsigned g = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n * dp, 256), c.sm_count * 16ull));
-  scale_pad_kernel<<<g, 256, 0, c.stream>>>(d_x, n, d, dp, sub, div, Y.get());
+  scale_pad_kernel<<<g, 256, 0, c.stream>>>(d_x, n, d, dp, sub, div, y);
   PM_LAUNCHED();
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
@@ -174,20 +181,23 @@ uint64_t scaled_column_means(Ctx& c, const float* d_x, uint64_t n, uint64_t d, f
   const cuuint64_t strides[1] = {static_cast<cuuint64_t>(dp) * 4};
   const cuuint32_t box[2] = {CQ_COLS, CQ_ROWS};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult cr = detail::get_encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, Y.get(), dims, strides, box, estr,
+  const CUresult cr = detail::get_encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, y, dims, strides, box, estr,
                                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   PM_REQUIRE(cr == CUDA_SUCCESS, PACMAP_ERR_CUDA, "cuTensorMapEncodeTiled (column sums) failed: " + std::to_string(cr));
   const size_t smem = 128 + static_cast<size_t>(CQ_STAGES) * CQ_ROWS * CQ_COLS * 4 + sizeof(CqShared);
   PM_CUDA(cudaFuncSetAttribute(colsum_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  colsum_chain_kernel<<<static_cast<unsigned>(dp / CQ_COLS), 64, smem, c.stream>>>(map, n, d, d_mean, c.d_err);
+  colsum_chain_kernel<<<static_cast<unsigned>(ceil_div(d, static_cast<uint64_t>(CQ_COLS))), 64, smem, c.stream>>>(
+      map, n, d, d_mean, c.d_err);
   PM_LAUNCHED();
-  return dp;
+  dp_out = dp;
+  return y;
 }
 
 void column_mean_seq(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float sub, float div, float* d_mean) {
   DevBuf<float> Y;
-  scaled_column_means(c, d_x, n, d, sub, div, Y, d_mean);
+  uint64_t dp = 0;
+  scaled_column_means(c, d_x, n, d, sub, div, nullptr, Y, d_mean, dp);
 }
 
 void preprocess_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float* d_out, float* h_min, float* h_max,
@@ -219,9 +229,10 @@ void preprocess_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float* 
     mean = mean_local.get();
   }
   DevBuf<float> Y;
-  const uint64_t dp = scaled_column_means(c, d_x, n, d, mn, mx, Y, mean);
+  uint64_t dp = 0;
+  const float* y = scaled_column_means(c, d_x, n, d, mn, mx, d_out, Y, mean, dp);  // y is d_out when d % 4 == 0
   const unsigned g2 = static_cast<unsigned>(std::min<uint64_t>(ceil_div(total, 256), c.sm_count * 16ull));
-  normalize_center_kernel<<<g2, 256, 0, c.stream>>>(Y.get(), n, d, dp, mean, d_out);
+  normalize_center_kernel<<<g2, 256, 0, c.stream>>>(y, n, d, dp, mean, d_out);
   PM_LAUNCHED();
 }
 
