@@ -68,70 +68,6 @@ struct alignas(8) TcShared {
 // Per-row candidate buffer maintenance (shared by the filter's compaction and the re-rank).
 // ---------------------------------------------------------------------------------------------
 
-// Rank-`rank` (1-based) smallest of total_key(u[0..m)) by a 4-pass 8-bit radix select, one warp.
-__device__ __forceinline__ uint32_t warp_radix_select(const float* __restrict__ u, int m, int rank, uint32_t* hist) {
-  const int lane = threadIdx.x & 31;
-  uint32_t prefix = 0, mask = 0;
-  int need = rank;
-#pragma unroll 1
-  for (int pass = 0; pass < 4; ++pass) {
-    const int shift = 24 - 8 * pass;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) hist[lane * 8 + b] = 0;
-    __syncwarp();
-    for (int e = lane; e < m; e += 32) {
-      const uint32_t key = total_key(u[e]);
-      if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
-    }
-    __syncwarp();
-    uint32_t local[8], lsum = 0;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      local[b] = hist[lane * 8 + b];
-      lsum += local[b];
-    }
-    uint32_t incl = lsum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    const uint32_t excl = incl - lsum;
-    // the lane whose bins contain the `need`-th element
-    const bool mine = (excl < static_cast<uint32_t>(need)) && (static_cast<uint32_t>(need) <= incl);
-    const unsigned who = __ballot_sync(0xFFFFFFFFu, mine);
-    const int src = who ? (__ffs(who) - 1) : 31;
-    int bin = 0;
-    uint32_t before = 0;
-    if (mine) {
-      uint32_t run = excl;
-#pragma unroll
-      for (int b = 0; b < 8; ++b) {
-        if (run + local[b] >= static_cast<uint32_t>(need)) {
-          bin = lane * 8 + b;
-          before = run;
-          break;
-        }
-        run += local[b];
-      }
-    }
-    bin = __shfl_sync(0xFFFFFFFFu, bin, src);
-    before = __shfl_sync(0xFFFFFFFFu, before, src);
-    prefix |= static_cast<uint32_t>(bin) << shift;
-    mask |= 255u << shift;
-    need -= static_cast<int>(before);
-    __syncwarp();
-  }
-  return prefix;
-}
-
-// u = v + 4 e_j (the row-relative upper bound) for every buffered candidate, one warp.
-__device__ __forceinline__ void fill_upper_bounds(const uint32_t* __restrict__ idx, const float* __restrict__ v,
-                                                  float* __restrict__ u, int m, const float* __restrict__ e4) {
-  for (int e = threadIdx.x & 31; e < m; e += 32) u[e] = v[e] + __ldg(e4 + idx[e]);
-  __syncwarp();
-}
-
 // theta for row constants (n_i, e4_i = 4 e_i) and the selected UB key: v <= theta keeps every
 // candidate whose lower bound is within the (sqrt-tie-widened) k'-th upper bound.
 __device__ __forceinline__ float theta_from(uint32_t ukey, float n_i, float e4_i) {
@@ -141,25 +77,26 @@ __device__ __forceinline__ float theta_from(uint32_t ukey, float n_i, float e4_i
   return base + slack;
 }
 
-// Register-resident compaction of one row's buffer (m <= 32 * PER entries), one warp: the entries
-// are loaded once, the rank-`rank` smallest upper bound is found by a 4-pass 8-bit radix select on
-// the registers, entries with v <= theta survive (order kept) and are written back once.
+// Register-resident compaction of one row's buffer (m <= 32 * PER (index, v) entries), one warp: the
+// entries are loaded once with their upper bounds u = v + 4 e_j, the rank-`rank` smallest u is found
+// by a 4-pass 8-bit radix select on the registers, entries with v <= theta survive (order kept) and are
+// written back once.
 template <int PER>
-__device__ __forceinline__ int warp_compact_regs(uint32_t* __restrict__ idx, float* __restrict__ v,
-                                                 float* __restrict__ u, int m, int rank, float n_i, float e4_i,
-                                                 uint32_t* hist, float& theta_out) {
+__device__ __forceinline__ int warp_compact_regs(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
+                                                 const float2* __restrict__ ge, uint32_t* hist, float& theta_out) {
   const int lane = threadIdx.x & 31;
   uint32_t ri[PER];
-  float rv[PER], ru[PER];
+  float rv[PER];
   uint32_t rk[PER];
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
     const int e = q * 32 + lane;
     const bool in = e < m;
-    ri[q] = in ? idx[e] : 0u;
-    rv[q] = in ? v[e] : 0.0f;
-    ru[q] = in ? u[e] : 0.0f;
-    rk[q] = in ? total_key(ru[q]) : 0xFFFFFFFFu;
+    const uint2 cv = in ? cand[e] : make_uint2(0u, 0u);
+    ri[q] = cv.x;
+    rv[q] = __uint_as_float(cv.y);
+    // the candidate's upper bound u = v + 4 e_j (e_j of its column)
+    rk[q] = in ? total_key(rv[q] + __ldg(&ge[ri[q]].y)) : 0xFFFFFFFFu;
   }
   uint32_t prefix = 0, mask = 0;
   int need = rank;
@@ -218,9 +155,7 @@ __device__ __forceinline__ int warp_compact_regs(uint32_t* __restrict__ idx, flo
     const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
     if (keep) {
       const int pos = out + __popc(bal & ((1u << lane) - 1u));
-      idx[pos] = ri[q];
-      v[pos] = rv[q];
-      u[pos] = ru[q];
+      cand[pos] = make_uint2(ri[q], __float_as_uint(rv[q]));
     }
     out += __popc(bal);
   }
@@ -472,8 +407,7 @@ template <int KB, int PER>  // K blocks of 64 elements: KP = 64 * KB; candidate 
 __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const __grid_constant__ CUtensorMap hmap, const __grid_constant__ CUtensorMap gmap, uint64_t n, uint64_t n_pad,
     uint32_t idesc, const float2* __restrict__ ge, const float* __restrict__ nrm, const uint32_t* __restrict__ perm,
-    int rank, uint32_t* __restrict__ cand_idx, float* __restrict__ cand_v, float* __restrict__ cand_u,
-    int* __restrict__ cand_cnt, uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow,
+    int rank, uint2* __restrict__ cand, int* __restrict__ cand_cnt, uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow,
     uint32_t* __restrict__ err) {
   constexpr int C = 32 * PER;
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
@@ -612,8 +546,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const float e4_i = valid ? ge[row].y : 0.0f;
     const uint64_t cbase = row * static_cast<uint64_t>(C);
     bool ok = true;
-    // e4v: this lane's 4 e_j for column colb + lane; an insertion at column c takes lane c's value.
-    auto screen = [&](const uint32_t (&r)[32], int colb, float e4v) {
+    auto screen = [&](const uint32_t (&r)[32], int colb) {
       float m8[4];
 #pragma unroll
       for (int g = 0; g < 4; ++g) {
@@ -627,12 +560,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
           if (__any_sync(0xFFFFFFFFu, -2.0f * m8[g] <= theta)) {
 #pragma unroll
             for (int c = 8 * g; c < 8 * g + 8; ++c) {
-              const float e4j = __shfl_sync(0xFFFFFFFFu, e4v, c);
               const float v = -2.0f * __uint_as_float(r[c]);
               if (v <= theta) {
-                cand_idx[cbase + cnt] = static_cast<uint32_t>(colb + c);
-                cand_v[cbase + cnt] = v;
-                cand_u[cbase + cnt] = v + e4j;
+                cand[cbase + cnt] = make_uint2(static_cast<uint32_t>(colb + c), __float_as_uint(v));
                 ++cnt;
               }
             }
@@ -640,23 +570,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         }
       }
     };
-    // The 4 e_j of each tile are loaded one tile ahead (coalesced), so an insertion never waits on memory.
-    float e4n[4];
-    {
-      const int c0n = sweep_tile(0, static_cast<int>(blockIdx.x), ntiles) * TC_BN;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) e4n[q] = __ldg(&ge[c0n + 32 * q + lane].y);
-    }
     for (int t = 0; t < ntiles; ++t) {
       const int acc = t & 1;
-      float e4c[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) e4c[q] = e4n[q];
-      if (t + 1 < ntiles) {
-        const int c0n = sweep_tile(t + 1, static_cast<int>(blockIdx.x), ntiles) * TC_BN;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) e4n[q] = __ldg(&ge[c0n + 32 * q + lane].y);
-      }
       if (!mbar_wait(&sh->tmem_full[acc], (t >> 1) & 1, abort_flag)) {
         ok = false;
         break;
@@ -671,8 +586,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         tmem_ld32_issue(taddr + cp * 64 + 32, r1);
         tmem_wait_ld_tied(r0);
         tie_regs(r1);
-        screen(r0, col0 + cp * 64, e4c[2 * cp]);
-        screen(r1, col0 + cp * 64 + 32, e4c[2 * cp + 1]);
+        screen(r0, col0 + cp * 64);
+        screen(r1, col0 + cp * 64 + 32);
       }
       tc_fence_before();
       __syncwarp();
@@ -687,7 +602,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         const float nL = __shfl_sync(0xFFFFFFFFu, n_i, L);
         const float eL = __shfl_sync(0xFFFFFFFFu, e4_i, L);
         float th;
-        const int kept = warp_compact_regs<PER>(cand_idx + rb, cand_v + rb, cand_u + rb, m, min(rank, m), nL, eL, hist, th);
+        const int kept = warp_compact_regs<PER>(cand + rb, m, min(rank, m), nL, eL, ge, hist, th);
         if (lane == L) {
           theta = th;
           cnt = kept;
@@ -723,8 +638,8 @@ constexpr int RC_WARPS = 4;
 
 template <int PER>
 __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
-    uint64_t n, int rank, const float* __restrict__ nrm, const float2* __restrict__ ge, uint32_t* __restrict__ cand_idx,
-    float* __restrict__ cand_v, float* __restrict__ cand_u, int* __restrict__ cand_cnt) {
+    uint64_t n, int rank, const float* __restrict__ nrm, const float2* __restrict__ ge, uint2* __restrict__ cand,
+    int* __restrict__ cand_cnt) {
   constexpr int C = 32 * PER;
   __shared__ uint32_t hist_all[RC_WARPS][256];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -735,8 +650,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     if (m0 <= 0) continue;
     const uint64_t rb = r * static_cast<uint64_t>(C);
     float th;
-    const int m = warp_compact_regs<PER>(cand_idx + rb, cand_v + rb, cand_u + rb, m0, min(rank, m0), nrm[r], ge[r].y,
-                                         hist, th);
+    const int m = warp_compact_regs<PER>(cand + rb, m0, min(rank, m0), nrm[r], ge[r].y, ge, hist, th);
     if (lane == 0) cand_cnt[r] = m;
   }
 }
@@ -747,7 +661,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
 template <int PER, int WARPS, int NC>
 __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
     const float* __restrict__ x, uint64_t n, int d, int K, const uint32_t* __restrict__ perm,
-    const uint32_t* __restrict__ cand_idx, const int* __restrict__ cand_cnt, uint32_t* __restrict__ out_idx,
+    const uint2* __restrict__ cand, const int* __restrict__ cand_cnt, uint32_t* __restrict__ out_idx,
     float* __restrict__ out_dist, uint32_t* __restrict__ fallback_rows, uint32_t* __restrict__ n_fallback) {
   constexpr int C = 32 * PER;
   __shared__ uint64_t keys_all[WARPS][C];
@@ -768,7 +682,7 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
     int nk = 0;
     for (int e0 = 0; e0 < m; e0 += 4) {
       const int e = e0 + grp;
-      const uint32_t jp = (e < m) ? cand_idx[rb + e] : static_cast<uint32_t>(r);
+      const uint32_t jp = (e < m) ? cand[rb + e].x : static_cast<uint32_t>(r);
       const uint32_t j = perm[jp];
       const float* b = x + static_cast<uint64_t>(j) * d;
       float accl = 0.0f;
@@ -904,8 +818,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
                                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   PM_REQUIRE(gr == CUDA_SUCCESS, PACMAP_ERR_CUDA, "cuTensorMapEncodeTiled (column term) failed: " + std::to_string(gr));
 
-  DevBuf<uint32_t> cidx(c, n_pad * C);
-  DevBuf<float> cv(c, n_pad * C), cu(c, n_pad * C);
+  DevBuf<uint2> cand(c, n_pad * C);
   DevBuf<int> ccnt(c, n_pad);
   DevBuf<uint32_t> ovf(c, n + 1), fbk(c, n + 1);
   PM_CUDA(cudaMemsetAsync(ccnt.get(), 0xFF, n_pad * sizeof(int), c.stream));
@@ -922,8 +835,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_CUDA(cudaEventRecord(ev[0], c.stream));
   auto launch = [&](auto kern) {
     PM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, idesc, ge.get(), nrm.get(), perm.get(), rank, cidx.get(),
-                                             cv.get(), cu.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err);
+    kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, idesc, ge.get(), nrm.get(), perm.get(), rank, cand.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err);
   };
   if (KB == 1 && PER == 16) launch(knn_filter_kernel<1, 16>);
   else if (KB == 1) launch(knn_filter_kernel<1, 32>);
@@ -940,28 +852,26 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
 
   const unsigned cgrid = std::min<unsigned>(ceil_div(n, RC_WARPS), c.sm_count * 16);
   if (PER == 16)
-    knn_compact_kernel<16><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cidx.get(), cv.get(),
-                                                                  cu.get(), ccnt.get());
+    knn_compact_kernel<16><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get());
   else
-    knn_compact_kernel<32><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cidx.get(), cv.get(),
-                                                                  cu.get(), ccnt.get());
+    knn_compact_kernel<32><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get());
   PM_LAUNCHED();
   const int di = static_cast<int>(d), ki = static_cast<int>(kp);
   if (PER == 16) {
     const unsigned rgrid = std::min<unsigned>(ceil_div(n, 8), c.sm_count * 32);
     if (d > 64)
-      knn_rerank_kernel<16, 8, 16><<<rgrid, 256, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cidx.get(), ccnt.get(), d_idx,
+      knn_rerank_kernel<16, 8, 16><<<rgrid, 256, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
                                                                 d_dist, fbk.get(), fbk.get() + n);
     else
-      knn_rerank_kernel<16, 8, 8><<<rgrid, 256, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cidx.get(), ccnt.get(), d_idx,
+      knn_rerank_kernel<16, 8, 8><<<rgrid, 256, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
                                                                d_dist, fbk.get(), fbk.get() + n);
   } else {
     const unsigned rgrid = std::min<unsigned>(ceil_div(n, 4), c.sm_count * 32);
     if (d > 64)
-      knn_rerank_kernel<32, 4, 16><<<rgrid, 128, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cidx.get(), ccnt.get(), d_idx,
+      knn_rerank_kernel<32, 4, 16><<<rgrid, 128, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
                                                                 d_dist, fbk.get(), fbk.get() + n);
     else
-      knn_rerank_kernel<32, 4, 8><<<rgrid, 128, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cidx.get(), ccnt.get(), d_idx,
+      knn_rerank_kernel<32, 4, 8><<<rgrid, 128, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
                                                                d_dist, fbk.get(), fbk.get() + n);
   }
   PM_LAUNCHED();
