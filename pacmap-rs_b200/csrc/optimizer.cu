@@ -7,7 +7,7 @@
 //    lists it (the squared distance and the weight use |y_i - y_j| only), so the sorted segments fix
 //    one deterministic summation order with no floating-point atomics. (The reference's rayon reduce,
 //    gradient.rs:53-70, has no fixed order at all.)
-// K8 grad_adam_kernel: one group of G lanes per point sums its segments (NN c=10, MN c=10000, FP
+// K8 grad_adam_kernel: one group of G = 8 lanes per point sums its segments (NN c=10, MN c=10000, FP
 //    repulsive c=1, exactly the per-pair f32 arithmetic of gradient.rs:120-147), reduces across the
 //    group in a fixed butterfly, and applies the Adam step (adam.rs:45-57) to that point at once:
 //    y is ping-ponged between two buffers because other points read y_j during the iteration.
@@ -561,7 +561,7 @@ void optimize_device(Ctx& c, const Csr& csr, const OptimizeArgs& a) {
   const uint64_t n = a.n, dim = a.dim;
   if (a.itr_end <= a.itr_begin || n == 0 || dim == 0) return;
   PM_REQUIRE(dim <= 8, PACMAP_ERR_UNSUPPORTED, "the optimiser supports embedding dimensions 1..8");
-  constexpr int G = 16;
+  constexpr int G = 8;
   GradFn fn = pick_grad_kernel<G>(dim);
   const uint64_t total_iters = a.p1 + a.p2 + a.p3;
   const uint64_t sched_len = std::max<uint64_t>(total_iters, a.itr_end);
@@ -640,7 +640,7 @@ void gradient_device(Ctx& c, const Csr& csr, const float* d_y, uint64_t n, uint6
                      float w_fp, float* d_grad, float* h_loss) {
   if (n == 0 || dim == 0) return;
   PM_REQUIRE(dim <= 8, PACMAP_ERR_UNSUPPORTED, "the optimiser supports embedding dimensions 1..8");
-  constexpr int G = 16;
+  constexpr int G = 8;
   GradFn fn = pick_grad_kernel<G>(dim);
   const Sched hs{w_nn, w_mn, w_fp, 0.0f};
   DevBuf<Sched> sched(c, 1);
