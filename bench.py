@@ -154,10 +154,18 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def _optimize_bytes(n, dim, iters, k=10, n_mn=5, n_fp=20):
+def _pair_counts(n, mid_near_ratio=0.5, far_pair_ratio=2.0):
+    """decide_num_pairs (lib.rs:565-597) in f32: (k, n_mn, n_fp)."""
+    rnd = lambda v: int(np.floor(np.float32(v) + np.float32(0.5)))  # noqa: E731  (f32::round: half away from 0)
+    k = 10 if n <= 10000 else rnd(np.float32(10.0) + np.float32(15.0) * (np.log10(np.float32(n)) - np.float32(4.0)))
+    return k, rnd(np.float32(k) * np.float32(mid_near_ratio)), rnd(np.float32(k) * np.float32(far_pair_ratio))
+
+
+def _optimize_bytes(n, dim, iters):
     """Algorithmic HBM bytes of the gradient + Adam iterations: 8 B per active pair (its two u32
     endpoints, read once), 4*n*dim for y read by the gradient, 24*n*dim for Adam (y, m, v read+write);
     mid-near pairs are inactive in phase 3 (w_mn = 0)."""
+    k, n_mn, n_fp = _pair_counts(n)
     p12 = n * (k + n_mn + n_fp)
     p3 = n * (k + n_fp)
     per = lambda pairs: 8 * pairs + 28 * n * dim  # noqa: E731
@@ -337,7 +345,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline_optimizer": {"kernel": "grad_adam_kernel (CSR gradient + Adam, CUDA graph)", "bound": "hbm",
                                "achieved": round(opt_gbs, 1) if opt_gbs else None, "peak": hbm, "unit": "GB/s",
                                "frac": round(opt_gbs / hbm, 4) if opt_gbs else None,
-                               "algorithmic": "8 B per active pair + 28*n*dim B per iteration",
+                               "algorithmic": "8 B per active pair + 28*n*dim B per iteration (k, n_mn, n_fp = %d, %d, %d)" % _pair_counts(n),
                                "peak_source": f"{src} HBM copy"},
         "clocks": clk.summary(),
     }
