@@ -15,7 +15,8 @@
 //     [LB, UB] = [v + n_i - 2e_i, v + 4e_j + n_i + 2e_i].
 //     Each row keeps a buffer of candidates with v <= theta_i, where theta_i comes from the (k'+1)-th
 //     smallest UB seen so far (the +1 covers the row itself); when the buffer fills, the owning warp
-//     compacts it with a radix select. Any true neighbour has LB <= k'-th UB, so it is never dropped.
+//     compacts it (the rank-th smallest upper bound by bisection on warp-wide counts). Any true
+//     neighbour has LB <= k'-th UB, so it is never dropped.
 //  3. knn_rerank_kernel: the final threshold, then the reference's exact f32 distance of every
 //     survivor, sorted by (distance, index): the rows of knn.rs.
 //  Rows whose candidate band does not fit the buffer (e.g. thousands of exact duplicates) are
@@ -58,7 +59,6 @@ struct alignas(8) TcShared {
   uint64_t mma_done;
   uint32_t tmem_base;
   int abort_flag;
-  uint32_t hist[TC_EPI_WARPS][256];
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -79,11 +79,10 @@ __device__ __forceinline__ float theta_from(uint32_t ukey, float n_i, float e4_i
 
 // Register-resident compaction of one row's buffer (m <= 32 * PER (index, v) entries), one warp: the
 // entries are loaded once with their upper bounds u = v + 4 e_j, the rank-`rank` smallest u is found
-// by a 4-pass 8-bit radix select on the registers, entries with v <= theta survive (order kept) and are
-// written back once.
+// by bisection on the registers, entries with v <= theta survive (order kept) and are written back once.
 template <int PER>
 __device__ __forceinline__ int warp_compact_regs(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
-                                                 const float2* __restrict__ ge, uint32_t* hist, float& theta_out) {
+                                                 const float2* __restrict__ ge, float& theta_out) {
   const int lane = threadIdx.x & 31;
   uint32_t ri[PER];
   float rv[PER];
@@ -98,55 +97,27 @@ __device__ __forceinline__ int warp_compact_regs(uint2* __restrict__ cand, int m
     // the candidate's upper bound u = v + 4 e_j (e_j of its column)
     rk[q] = in ? total_key(rv[q] + __ldg(&ge[ri[q]].y)) : 0xFFFFFFFFu;
   }
-  uint32_t prefix = 0, mask = 0;
-  int need = rank;
-#pragma unroll 1
-  for (int pass = 0; pass < 4; ++pass) {
-    const int shift = 24 - 8 * pass;
+  // The rank-th smallest key by bisection on [min key, max key] with warp-wide counts (no shared
+  // memory, no atomics): the smallest key value T with #{keys <= T} >= rank.
+  uint32_t kmin = 0xFFFFFFFFu, kmax = 0u;
 #pragma unroll
-    for (int b = 0; b < 8; ++b) hist[lane * 8 + b] = 0;
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < PER; ++q)
-      if (q * 32 + lane < m && (rk[q] & mask) == prefix) atomicAdd(&hist[(rk[q] >> shift) & 255u], 1u);
-    __syncwarp();
-    uint32_t local[8], lsum = 0;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      local[b] = hist[lane * 8 + b];
-      lsum += local[b];
+  for (int q = 0; q < PER; ++q) {
+    if (q * 32 + lane < m) {
+      kmin = min(kmin, rk[q]);
+      kmax = max(kmax, rk[q]);
     }
-    uint32_t incl = lsum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    const uint32_t excl = incl - lsum;
-    const bool mine = (excl < static_cast<uint32_t>(need)) && (static_cast<uint32_t>(need) <= incl);
-    const unsigned who = __ballot_sync(0xFFFFFFFFu, mine);
-    const int src = who ? (__ffs(who) - 1) : 31;
-    int bin = 0;
-    uint32_t before = 0;
-    if (mine) {
-      uint32_t run = excl;
-#pragma unroll
-      for (int b = 0; b < 8; ++b) {
-        if (run + local[b] >= static_cast<uint32_t>(need)) {
-          bin = lane * 8 + b;
-          before = run;
-          break;
-        }
-        run += local[b];
-      }
-    }
-    bin = __shfl_sync(0xFFFFFFFFu, bin, src);
-    before = __shfl_sync(0xFFFFFFFFu, before, src);
-    prefix |= static_cast<uint32_t>(bin) << shift;
-    mask |= 255u << shift;
-    need -= static_cast<int>(before);
-    __syncwarp();
   }
+  uint32_t lo = __reduce_min_sync(0xFFFFFFFFu, kmin), hi = __reduce_max_sync(0xFFFFFFFFu, kmax);
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) cnt += (q * 32 + lane < m && rk[q] <= mid) ? 1u : 0u;
+    cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
+    if (cnt >= static_cast<uint32_t>(rank)) hi = mid;
+    else lo = mid + 1u;
+  }
+  const uint32_t prefix = lo;
   const float th = theta_from(prefix, n_i, e4_i);
   int out = 0;
 #pragma unroll
@@ -539,7 +510,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const int quad = warp & 3;  // TMEM lane quadrant this warp may access
     const uint64_t row = row0 + half * 128 + quad * 32 + lane;
     const bool valid = row < n;
-    uint32_t* hist = sh->hist[ew];
     float theta = valid ? 3.402823466e+38f : -__int_as_float(0x7f800000);
     int cnt = 0;
     const float n_i = valid ? nrm[row] : 0.0f;
@@ -602,7 +572,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         const float nL = __shfl_sync(0xFFFFFFFFu, n_i, L);
         const float eL = __shfl_sync(0xFFFFFFFFu, e4_i, L);
         float th;
-        const int kept = warp_compact_regs<PER>(cand + rb, m, min(rank, m), nL, eL, ge, hist, th);
+        const int kept = warp_compact_regs<PER>(cand + rb, m, min(rank, m), nL, eL, ge, th);
         if (lane == L) {
           theta = th;
           cnt = kept;
@@ -641,16 +611,14 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     uint64_t n, int rank, const float* __restrict__ nrm, const float2* __restrict__ ge, uint2* __restrict__ cand,
     int* __restrict__ cand_cnt) {
   constexpr int C = 32 * PER;
-  __shared__ uint32_t hist_all[RC_WARPS][256];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* hist = hist_all[warp];
   for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * RC_WARPS + warp; r < n;
        r += static_cast<uint64_t>(gridDim.x) * RC_WARPS) {
     const int m0 = min(cand_cnt[r], C);
     if (m0 <= 0) continue;
     const uint64_t rb = r * static_cast<uint64_t>(C);
     float th;
-    const int m = warp_compact_regs<PER>(cand + rb, m0, min(rank, m0), nrm[r], ge[r].y, ge, hist, th);
+    const int m = warp_compact_regs<PER>(cand + rb, m0, min(rank, m0), nrm[r], ge[r].y, ge, th);
     if (lane == 0) cand_cnt[r] = m;
   }
 }
