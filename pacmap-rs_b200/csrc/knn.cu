@@ -166,7 +166,7 @@ void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t
     if (knn_tc_device(c, d_x, n, d, kp, mode == PACMAP_KNN_TENSOR_BF16, d_idx, d_dist)) return;
   }
   PM_REQUIRE(mode == PACMAP_KNN_AUTO || mode == PACMAP_KNN_SIMT_EXACT, PACMAP_ERR_UNSUPPORTED,
-             "the tensor-core kNN does not support this shape (d <= 128 and k' <= 192 are required)");
+             "the tensor-core kNN does not support this shape (d <= 1024 and k' <= 447 are required)");
   knn_rows_simt(c, d_x, n, d, kp, nullptr, n, d_idx, d_dist);
 }
 

@@ -43,7 +43,7 @@ namespace {
 
 constexpr int TC_BM = 256;         // rows per block (two M = 128 accumulators)
 constexpr int TC_BN = 128;         // columns per tile (MMA N)
-constexpr int TC_STAGES = 4;       // B-operand pipeline depth
+constexpr int TC_MAX_STAGES = 8;   // operand pipeline depth limit (mbarrier slots)
 constexpr int TC_THREADS = 320;    // warp 0 TMA, warp 1 MMA + TMEM owner, warps 2..9 epilogue
 constexpr int TC_EPI_WARPS = 8;
 constexpr int TC_TMEM_COLS = 512;  // 2 accumulator stages x 2 halves x 128 columns
@@ -51,14 +51,34 @@ constexpr int KB_BYTES = 128 * 128;  // one 128-row x 64-element (128 B) swizzle
 constexpr int G_BYTES = 128 * 32;    // one 128-row x 16-element (32 B) column-term tile
 
 struct alignas(8) TcShared {
-  uint64_t full[TC_STAGES];
-  uint64_t empty[TC_STAGES];
+  uint64_t full[TC_MAX_STAGES];
+  uint64_t empty[TC_MAX_STAGES];
   uint64_t a_full;
   uint64_t tmem_full[2];
   uint64_t tmem_empty[2];
   uint64_t mma_done;
   uint32_t tmem_base;
   int abort_flag;
+};
+
+// Operand staging of the filter by data width (KB = K blocks of 64 elements):
+//  MODE_TILE   (KB <= 2): the block's A rows stay in shared memory; one stage = every K block of a
+//              column tile.
+//  MODE_KBLOCK (KB 3..4): A stays resident; one stage = one K block of a column tile.
+//  MODE_STREAM (KB >= 5): A no longer fits; one stage = one K block of both A halves and of the column
+//              tile (A is re-read from L2 for every tile). KB is a run-time value here.
+// The column-term tile rides with the first stage of each column tile.
+enum FilterMode { MODE_TILE = 0, MODE_KBLOCK = 1, MODE_STREAM = 2 };
+constexpr int TC_SMEM_LIMIT = 232448;  // 227 KB of dynamic shared memory per block
+template <int KB, int MODE>
+struct FilterLayout {
+  static constexpr int A_RES = MODE == MODE_STREAM ? 0 : 2 * KB * KB_BYTES;
+  static constexpr int STAGE = (MODE == MODE_TILE ? KB : 1) * KB_BYTES + (MODE == MODE_STREAM ? 2 * KB_BYTES : 0);
+  static constexpr int FIT = (TC_SMEM_LIMIT - 1024 - A_RES - G_BYTES - 256) / (STAGE + G_BYTES);
+  static constexpr int NST = MODE == MODE_TILE ? 4 : (FIT > TC_MAX_STAGES ? TC_MAX_STAGES : FIT);
+  static constexpr size_t SMEM = 1024 + A_RES + static_cast<size_t>(NST + 1) * G_BYTES +
+                                 static_cast<size_t>(NST) * STAGE + sizeof(TcShared);
+  static_assert(NST >= 2 && SMEM <= TC_SMEM_LIMIT, "filter operands do not fit in shared memory");
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -374,24 +394,30 @@ __global__ void bound_kernel(uint64_t n, uint64_t n_pad, int d, int KP, float rh
 // ---------------------------------------------------------------------------------------------
 // 2. the tcgen05 filter
 // ---------------------------------------------------------------------------------------------
-template <int KB, int PER>  // K blocks of 64 elements: KP = 64 * KB; candidate buffer C = 32 * PER
+// K blocks of 64 elements: KP = 64 * KB (KB = 0: run-time kb_rt, MODE_STREAM only); candidate buffer
+// C = 32 * PER per row.
+template <int KB, int PER, int MODE>
 __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const __grid_constant__ CUtensorMap hmap, const __grid_constant__ CUtensorMap gmap, uint64_t n, uint64_t n_pad,
-    uint32_t idesc, const float2* __restrict__ ge, const float* __restrict__ nrm, const uint32_t* __restrict__ perm,
-    int rank, uint2* __restrict__ cand, int* __restrict__ cand_cnt, uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow,
-    uint32_t* __restrict__ err) {
+    int kb_rt, uint32_t idesc, const float2* __restrict__ ge, const float* __restrict__ nrm,
+    const uint32_t* __restrict__ perm, int rank, uint2* __restrict__ cand, int* __restrict__ cand_cnt,
+    uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err) {
+  using L = FilterLayout<KB, MODE>;
+  constexpr int NST = L::NST;
   constexpr int C = 32 * PER;
+  const int nkb = KB > 0 ? KB : kb_rt;
+  const int nch = MODE == MODE_TILE ? 1 : nkb;  // stages per column tile
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-  // 1024-byte aligned operand region: A [2 halves][KB][16 KB], the all-ones tile [4 KB], the
-  // column-term tiles [STAGES][4 KB], B [STAGES][KB][16 KB], then TcShared (the small tiles sit below
-  // the large B stages).
+  // 1024-byte aligned operand region: resident A [2 halves][KB][16 KB] (not in MODE_STREAM), the
+  // all-ones tile [4 KB], the column-term tiles [NST][4 KB], the stages [NST][L::STAGE], then TcShared.
+  // Inside a stage: the column tile's K block(s) first, then (MODE_STREAM) the two A halves' K block.
   // aligned by offsetting the shared array itself, so every access keeps the shared address space
   unsigned char* base = tc_smem_raw + ((1024u - (smem_u32(tc_smem_raw) & 1023u)) & 1023u);
   unsigned char* a_smem = base;
-  unsigned char* one_smem = base + 2 * KB * KB_BYTES;
+  unsigned char* one_smem = base + L::A_RES;
   unsigned char* g_smem = one_smem + G_BYTES;
-  unsigned char* b_smem = g_smem + TC_STAGES * G_BYTES;
-  TcShared* sh = reinterpret_cast<TcShared*>(b_smem + TC_STAGES * KB * KB_BYTES);
+  unsigned char* st_smem = g_smem + NST * G_BYTES;
+  TcShared* sh = reinterpret_cast<TcShared*>(st_smem + NST * L::STAGE);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t row0 = static_cast<uint64_t>(blockIdx.x) * TC_BM;
@@ -401,9 +427,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
   for (int e = threadIdx.x; e < G_BYTES / 4; e += TC_THREADS) reinterpret_cast<uint32_t*>(one_smem)[e] = 0x3F803F80u;
   fence_proxy_async_smem();
   if (threadIdx.x == 0) {
-    for (int s = 0; s < TC_STAGES; ++s) {
-      mbar_init(&sh->full[s], 1);
-      mbar_init(&sh->empty[s], 1);
+    for (int q = 0; q < NST; ++q) {
+      mbar_init(&sh->full[q], 1);
+      mbar_init(&sh->empty[q], 1);
     }
     mbar_init(&sh->a_full, 1);
     for (int a = 0; a < 2; ++a) {
@@ -428,67 +454,104 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
   if (warp == 0) {
     // ------------------------------- TMA producer -------------------------------
     if (lane == 0) {
-      mbar_expect_tx(&sh->a_full, 2 * KB * KB_BYTES);
-      for (int h = 0; h < 2; ++h)
-        for (int kb = 0; kb < KB; ++kb)
-          tma_load_2d(a_smem + (h * KB + kb) * KB_BYTES, &hmap, &sh->a_full, kb * 64, static_cast<int>(row0 + h * 128));
-      int issued = 0;
-      for (int t = 0; t < ntiles; ++t) {
-        const int s = t % TC_STAGES;
-        if (t >= TC_STAGES && !mbar_wait(&sh->empty[s], ((t / TC_STAGES) + 1) & 1, abort_flag)) break;
-        mbar_expect_tx(&sh->full[s], KB * KB_BYTES + G_BYTES);
-        const int tile = sweep_tile(t, static_cast<int>(blockIdx.x), ntiles);
-        for (int kb = 0; kb < KB; ++kb)
-          tma_load_2d(b_smem + (s * KB + kb) * KB_BYTES, &hmap, &sh->full[s], kb * 64, tile * TC_BN);
-        tma_load_2d(g_smem + s * G_BYTES, &gmap, &sh->full[s], 0, tile * TC_BN);
-        issued = t + 1;
+      if (MODE != MODE_STREAM) {
+        mbar_expect_tx(&sh->a_full, L::A_RES);
+        for (int h = 0; h < 2; ++h)
+          for (int kb = 0; kb < KB; ++kb)
+            tma_load_2d(a_smem + (h * KB + kb) * KB_BYTES, &hmap, &sh->a_full, kb * 64, static_cast<int>(row0 + h * 128));
       }
-      if (issued < ntiles) {
+      const int total = ntiles * nch;
+      int issued = 0, s = 0, ph = 0;
+      bool stop = false;
+      for (int t = 0; t < ntiles && !stop; ++t) {
+        const int tile = sweep_tile(t, static_cast<int>(blockIdx.x), ntiles);
+        for (int ch = 0; ch < nch; ++ch) {
+          if (issued >= NST && !mbar_wait(&sh->empty[s], ph ^ 1, abort_flag)) {
+            stop = true;
+            break;
+          }
+          unsigned char* st = st_smem + s * L::STAGE;
+          const uint32_t bytes = (MODE == MODE_TILE ? KB * KB_BYTES : KB_BYTES) +
+                                 (MODE == MODE_STREAM ? 2 * KB_BYTES : 0) + (ch == 0 ? G_BYTES : 0);
+          mbar_expect_tx(&sh->full[s], bytes);
+          if (MODE == MODE_TILE) {
+            for (int kb = 0; kb < KB; ++kb) tma_load_2d(st + kb * KB_BYTES, &hmap, &sh->full[s], kb * 64, tile * TC_BN);
+          } else {
+            tma_load_2d(st, &hmap, &sh->full[s], ch * 64, tile * TC_BN);
+            if (MODE == MODE_STREAM)
+              for (int h = 0; h < 2; ++h)
+                tma_load_2d(st + (1 + h) * KB_BYTES, &hmap, &sh->full[s], ch * 64, static_cast<int>(row0 + h * 128));
+          }
+          if (ch == 0) tma_load_2d(g_smem + s * G_BYTES, &gmap, &sh->full[s], 0, tile * TC_BN);
+          ++issued;
+          if (++s == NST) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+      }
+      if (issued < total) {
         atomicOr(err, DEV_ERR_TIMEOUT);
         sh->abort_flag = 1;
       }
       // Drain: every issued load has landed before the block may exit.
-      mbar_wait(&sh->a_full, 0, abort_flag);
-      for (int t = (issued > TC_STAGES ? issued - TC_STAGES : 0); t < issued; ++t) {
+      if (MODE != MODE_STREAM) mbar_wait(&sh->a_full, 0, abort_flag);
+      for (int q = (issued > NST ? issued - NST : 0); q < issued; ++q) {
         const uint64_t t0 = globaltimer();
-        while (!mbar_try_wait(&sh->full[t % TC_STAGES], (t / TC_STAGES) & 1) && globaltimer() - t0 < WAIT_LIMIT_NS) {
+        while (!mbar_try_wait(&sh->full[q % NST], (q / NST) & 1) && globaltimer() - t0 < WAIT_LIMIT_NS) {
         }
       }
     }
   } else if (warp == 1) {
     // ------------------------------- MMA issuer -------------------------------
     if (lane == 0) {
-      bool ok = mbar_wait(&sh->a_full, 0, abort_flag);
-      const uint32_t a_addr = smem_u32(a_smem), b_addr = smem_u32(b_smem), g_addr = smem_u32(g_smem);
+      bool ok = MODE == MODE_STREAM ? true : mbar_wait(&sh->a_full, 0, abort_flag);
+      const uint32_t a_addr = smem_u32(a_smem), st_addr = smem_u32(st_smem), g_addr = smem_u32(g_smem);
       const uint64_t ones = sdesc_sw32(smem_u32(one_smem));
       const uint32_t idesc_col = idesc_f16(true);  // the column term is bf16 x bf16
-      int t = 0;
-      for (; ok && t < ntiles; ++t) {
-        const int s = t % TC_STAGES, acc = t & 1;
-        if (!mbar_wait(&sh->full[s], (t / TC_STAGES) & 1, abort_flag)) {
-          ok = false;
-          break;
-        }
-        if (t >= 2 && !mbar_wait(&sh->tmem_empty[acc], ((t >> 1) + 1) & 1, abort_flag)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint64_t gd = sdesc_sw32(g_addr + s * G_BYTES);
+      int s = 0, ph = 0;
+      for (int t = 0; ok && t < ntiles; ++t) {
+        const int acc = t & 1;
+        for (int ch = 0; ch < nch; ++ch) {
+          if (!mbar_wait(&sh->full[s], ph, abort_flag)) {
+            ok = false;
+            break;
+          }
+          if (ch == 0 && t >= 2 && !mbar_wait(&sh->tmem_empty[acc], ((t >> 1) + 1) & 1, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = st_addr + s * L::STAGE;
+          const uint64_t gd = sdesc_sw32(g_addr + s * G_BYTES);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const uint32_t d_tmem = tmem + acc * 256 + h * 128;
-          // D = -g_j / 2 (rank-1: ones x the column term), then D += h_i . h_j
-          umma_f16(d_tmem, ones, gd, idesc_col, 0u);
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t d_tmem = tmem + acc * 256 + h * 128;
+            // D = -g_j / 2 (rank-1: ones x the column term), then D += h_i . h_j over the K blocks in order
+            if (ch == 0) umma_f16(d_tmem, ones, gd, idesc_col, 0u);
+            if (MODE == MODE_TILE) {
 #pragma unroll
-          for (int kb = 0; kb < KB; ++kb) {
-            const uint64_t ad = sdesc_sw128(a_addr + (h * KB + kb) * KB_BYTES);
-            const uint64_t bd = sdesc_sw128(b_addr + (s * KB + kb) * KB_BYTES);
+              for (int kb = 0; kb < KB; ++kb) {
+                const uint64_t ad = sdesc_sw128(a_addr + (h * KB + kb) * KB_BYTES);
+                const uint64_t bd = sdesc_sw128(st + kb * KB_BYTES);
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) umma_f16(d_tmem, ad + 2 * kk, bd + 2 * kk, idesc, 1u);
+                for (int kk = 0; kk < 4; ++kk) umma_f16(d_tmem, ad + 2 * kk, bd + 2 * kk, idesc, 1u);
+              }
+            } else {
+              const uint64_t ad = sdesc_sw128(MODE == MODE_STREAM ? st + (1 + h) * KB_BYTES
+                                                                  : a_addr + (h * KB + ch) * KB_BYTES);
+              const uint64_t bd = sdesc_sw128(st);
+#pragma unroll
+              for (int kk = 0; kk < 4; ++kk) umma_f16(d_tmem, ad + 2 * kk, bd + 2 * kk, idesc, 1u);
+            }
+          }
+          umma_commit(&sh->empty[s]);
+          if (++s == NST) {
+            s = 0;
+            ph ^= 1;
           }
         }
-        umma_commit(&sh->empty[s]);
+        if (!ok) break;
         umma_commit(&sh->tmem_full[acc]);
       }
       if (!ok) {
@@ -624,8 +687,9 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
 }
 
 // 3b. exact re-rank of the compacted band: the reference's f32 distance of every survivor (8-lane
-//     groups in distance.rs:50-75's lane order, 4 survivors per warp pass, row i of x in registers),
-//     sorted by (distance, index); output at the original row, original indices.
+//     groups in distance.rs:50-75's lane order, 4 survivors per warp pass, row i of x in registers
+//     when it has at most 8 * NC elements, else read from L1 each pass with NC = 0), sorted by
+//     (distance, index); output at the original row, original indices.
 template <int PER, int WARPS, int NC>
 __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
     const float* __restrict__ x, uint64_t n, int d, int K, const uint32_t* __restrict__ perm,
@@ -644,7 +708,7 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
     const uint64_t rb = r * static_cast<uint64_t>(C);
     const uint64_t orow = perm[r];
     const float* a = x + orow * d;
-    float ra[NC];
+    float ra[NC > 0 ? NC : 1];
 #pragma unroll
     for (int ch = 0; ch < NC; ++ch) ra[ch] = ch < nc ? a[8 * ch + l8] : 0.0f;
     int nk = 0;
@@ -654,10 +718,17 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
       const uint32_t j = perm[jp];
       const float* b = x + static_cast<uint64_t>(j) * d;
       float accl = 0.0f;
+      if (NC > 0) {
 #pragma unroll
-      for (int ch = 0; ch < NC; ++ch) {
-        if (ch < nc) {
-          const float df = __fsub_rn(ra[ch], b[8 * ch + l8]);
+        for (int ch = 0; ch < NC; ++ch) {
+          if (ch < nc) {
+            const float df = __fsub_rn(ra[ch], b[8 * ch + l8]);
+            accl = __fadd_rn(accl, __fmul_rn(df, df));
+          }
+        }
+      } else {
+        for (int ch = 0; ch < nc; ++ch) {
+          const float df = __fsub_rn(a[8 * ch + l8], b[8 * ch + l8]);
           accl = __fadd_rn(accl, __fmul_rn(df, df));
         }
       }
@@ -698,14 +769,15 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
 }  // namespace
 
 bool knn_tc_supported(uint64_t n, uint64_t d, uint64_t kp) {
-  return d >= 1 && d <= 128 && kp >= 1 && kp + 1 <= 448 && n >= 2 && n < (1ull << 31);
+  return d >= 1 && d <= 1024 && kp >= 1 && kp + 1 <= 448 && n >= 2 && n < (1ull << 31);
 }
 
 bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, bool bf16, uint32_t* d_idx,
                    float* d_dist) {
   if (!knn_tc_supported(n, d, kp)) return false;
-  const int KB = d <= 64 ? 1 : 2;
+  const int KB = static_cast<int>((d + 63) / 64);
   const int KP = 64 * KB;
+  const int mode = KB <= 2 ? MODE_TILE : (KB <= 4 ? MODE_KBLOCK : MODE_STREAM);
   const uint64_t n_pad = (n + TC_BM - 1) / TC_BM * TC_BM;
   const int PER = (kp + 1 <= 192) ? 16 : 32;  // buffer C = 512 or 1024 candidates per row
   const int C = 32 * PER;
@@ -793,22 +865,39 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_CUDA(cudaMemsetAsync(ovf.get() + n, 0, sizeof(uint32_t), c.stream));
   PM_CUDA(cudaMemsetAsync(fbk.get() + n, 0, sizeof(uint32_t), c.stream));
 
-  const size_t smem =
-      1024 + static_cast<size_t>(2 + TC_STAGES) * KB * KB_BYTES + (TC_STAGES + 1) * G_BYTES + sizeof(TcShared);
   const uint32_t idesc = idesc_f16(bf16);
   const unsigned grid = static_cast<unsigned>(n_pad / TC_BM);
   cudaEvent_t ev[2];
   PM_CUDA(cudaEventCreate(&ev[0]));
   PM_CUDA(cudaEventCreate(&ev[1]));
   PM_CUDA(cudaEventRecord(ev[0], c.stream));
-  auto launch = [&](auto kern) {
+  auto launch = [&](auto kern, size_t smem) {
     PM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, idesc, ge.get(), nrm.get(), perm.get(), rank, cand.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err);
+    kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, KB, idesc, ge.get(), nrm.get(), perm.get(), rank,
+                                               cand.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err);
   };
-  if (KB == 1 && PER == 16) launch(knn_filter_kernel<1, 16>);
-  else if (KB == 1) launch(knn_filter_kernel<1, 32>);
-  else if (PER == 16) launch(knn_filter_kernel<2, 16>);
-  else launch(knn_filter_kernel<2, 32>);
+  const bool p16 = PER == 16;
+  if (mode == MODE_STREAM) {
+    constexpr size_t sm = FilterLayout<0, MODE_STREAM>::SMEM;
+    if (p16) launch(knn_filter_kernel<0, 16, MODE_STREAM>, sm);
+    else launch(knn_filter_kernel<0, 32, MODE_STREAM>, sm);
+  } else if (KB == 1) {
+    constexpr size_t sm = FilterLayout<1, MODE_TILE>::SMEM;
+    if (p16) launch(knn_filter_kernel<1, 16, MODE_TILE>, sm);
+    else launch(knn_filter_kernel<1, 32, MODE_TILE>, sm);
+  } else if (KB == 2) {
+    constexpr size_t sm = FilterLayout<2, MODE_TILE>::SMEM;
+    if (p16) launch(knn_filter_kernel<2, 16, MODE_TILE>, sm);
+    else launch(knn_filter_kernel<2, 32, MODE_TILE>, sm);
+  } else if (KB == 3) {
+    constexpr size_t sm = FilterLayout<3, MODE_KBLOCK>::SMEM;
+    if (p16) launch(knn_filter_kernel<3, 16, MODE_KBLOCK>, sm);
+    else launch(knn_filter_kernel<3, 32, MODE_KBLOCK>, sm);
+  } else {
+    constexpr size_t sm = FilterLayout<4, MODE_KBLOCK>::SMEM;
+    if (p16) launch(knn_filter_kernel<4, 16, MODE_KBLOCK>, sm);
+    else launch(knn_filter_kernel<4, 32, MODE_KBLOCK>, sm);
+  }
   PM_LAUNCHED();
   PM_CUDA(cudaEventRecord(ev[1], c.stream));
   c.check_errors("tensor-core kNN filter");
@@ -825,22 +914,21 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     knn_compact_kernel<32><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get());
   PM_LAUNCHED();
   const int di = static_cast<int>(d), ki = static_cast<int>(kp);
+  auto rerank = [&](auto kern, int warps) {
+    const unsigned rgrid = std::min<unsigned>(ceil_div(n, warps), c.sm_count * 32);
+    kern<<<rgrid, warps * 32, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx, d_dist,
+                                             fbk.get(), fbk.get() + n);
+  };
   if (PER == 16) {
-    const unsigned rgrid = std::min<unsigned>(ceil_div(n, 8), c.sm_count * 32);
-    if (d > 64)
-      knn_rerank_kernel<16, 8, 16><<<rgrid, 256, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
-                                                                d_dist, fbk.get(), fbk.get() + n);
-    else
-      knn_rerank_kernel<16, 8, 8><<<rgrid, 256, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
-                                                               d_dist, fbk.get(), fbk.get() + n);
+    if (d > 256) rerank(knn_rerank_kernel<16, 8, 0>, 8);
+    else if (d > 128) rerank(knn_rerank_kernel<16, 8, 32>, 8);
+    else if (d > 64) rerank(knn_rerank_kernel<16, 8, 16>, 8);
+    else rerank(knn_rerank_kernel<16, 8, 8>, 8);
   } else {
-    const unsigned rgrid = std::min<unsigned>(ceil_div(n, 4), c.sm_count * 32);
-    if (d > 64)
-      knn_rerank_kernel<32, 4, 16><<<rgrid, 128, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
-                                                                d_dist, fbk.get(), fbk.get() + n);
-    else
-      knn_rerank_kernel<32, 4, 8><<<rgrid, 128, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
-                                                               d_dist, fbk.get(), fbk.get() + n);
+    if (d > 256) rerank(knn_rerank_kernel<32, 4, 0>, 4);
+    else if (d > 128) rerank(knn_rerank_kernel<32, 4, 32>, 4);
+    else if (d > 64) rerank(knn_rerank_kernel<32, 4, 16>, 4);
+    else rerank(knn_rerank_kernel<32, 4, 8>, 4);
   }
   PM_LAUNCHED();
 

@@ -19,7 +19,11 @@ def _mix(n, d, seed):
 
 @pytest.mark.parametrize("mode", [F16, BF16])
 @pytest.mark.parametrize("n,d,k", [(3001, 128, 90), (2000, 100, 60), (4096, 32, 17), (777, 13, 90), (300, 64, 10),
-                                   (1024, 128, 1), (513, 65, 200)])
+                                   (1024, 128, 1), (513, 65, 200),
+                                   # resident A, one K block per stage (d 129..256)
+                                   (700, 130, 17), (4100, 192, 99), (2000, 256, 90),
+                                   # A and B streamed per K block (d > 256), ragged last block included
+                                   (1000, 300, 60), (1500, 784, 72), (600, 1024, 30), (257, 333, 256)])
 def test_tc_knn_bit_exact(lib, orc, mode, n, d, k):
     x = _mix(n, d, seed=n + d)
     gi, gd = lib.knn.find_k_nearest_neighbors(x, k, knn_mode=mode)
@@ -60,3 +64,30 @@ def test_tc_knn_quantised_ties(lib, orc):
     gi, gd = lib.knn.find_k_nearest_neighbors(x, 72, knn_mode=F16)
     ei, ed = orc.knn_exact(x, 72)
     assert np.array_equal(gd, ed) and np.array_equal(gi, ei)
+
+
+def _tc_vs_simt(lib, x, k):
+    # the tensor-core path (AUTO at n >= 16384) against the exact SIMT path (mode 3), which the tests
+    # above and tests/test_gpu_parity.py pin to the oracle: indices and f32 distances bit-exact
+    gi, gd = lib.knn.find_k_nearest_neighbors(x, k, knn_mode=AUTO)
+    si, sd = lib.knn.find_k_nearest_neighbors(x, k, knn_mode=3)
+    assert np.array_equal(gd, sd)
+    assert np.array_equal(gi, si)
+
+
+def test_tc_knn_image_like_60k_x_784(lib):
+    # the 60,000 x 784 image-like configuration (quantised to 1/255, many ties), k' = 22 + 50
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.image_like(n=60000, d=784, seed=0)
+    xp = lib.stages.preprocess(x)[0]
+    _tc_vs_simt(lib, xp, 72)
+
+
+def test_tc_knn_subspace_mixture_slice_256(lib):
+    # a 100,000-row draw of the 4M x 256 subspace-mixture generator, k' = 49 + 50
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.subspace_mixture(n=100000, d=256, seed=2)
+    xp = lib.stages.preprocess(x)[0]
+    _tc_vs_simt(lib, xp, 99)
