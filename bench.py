@@ -1,6 +1,7 @@
 """Benchmark: seconds to embed a 1,000,000 x 128 mixture with PaCMAP on B200 (one JSON line).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n ROWS] [--d COLS]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload 1m-128|4m-256]
+                    [--n ROWS] [--d COLS]
 
 A learned initialiser (MLP 128-512-512-2) is first trained, outside the timed region, on the plain GPU
 embedding of 200,000 draws of the generator. One step = one full learned-init fit_transform of a fresh
@@ -17,6 +18,8 @@ With N GPUs (torchrun) every rank embeds its own dataset (replicas only: the pat
 timing is the max over ranks and value is seconds per embedding for the whole job.
 `--impl reference` times the CPU restatement of the reference (the reference's Rust crate cannot be
 built here) on a bounded sample on rank 0 and projects it to the full size.
+`--workload 4m-256` runs the large configuration instead: 4,000,000 x 256 draws of a 200-Gaussian
+mixture on a 32-dim subspace (noise 0.05 elsewhere) -> 3-D, MLP 256-512-512-3 trained on 300,000 draws.
 """
 from __future__ import annotations
 
@@ -35,6 +38,15 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "pacmap-rs_b200"))
 
 METRIC = "s to embed 1M×128 at matched 10-NN preservation, learned-init vs plain GPU"
+WORKLOADS = {
+    "1m-128": {"n": 1_000_000, "d": 128, "dim": 2, "n_train": 200_000, "generator": "anisotropic",
+               "metric": METRIC,
+               "generator_desc": "anisotropic 50-Gaussian mixture (seed 0; draw seed 1000+rank)"},
+    "4m-256": {"n": 4_000_000, "d": 256, "dim": 3, "n_train": 300_000, "generator": "subspace",
+               "metric": "s to embed 4M×256 -> 3-D at matched 10-NN preservation, learned-init vs plain GPU",
+               "generator_desc": ("200 Gaussians on a random 32-dim subspace + N(0, 0.05^2) in the other dims "
+                                  "(seed 0; draw seed 1000+rank)")},
+}
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -90,11 +102,14 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def make_data(n, d, seed, draw_seed=None):
-    """n draws of the anisotropic 50-Gaussian mixture fixed by `seed` (fresh points per `draw_seed`)."""
+def make_data(n, d, seed, draw_seed=None, generator="anisotropic"):
+    """n draws of the workload's mixture fixed by `seed` (fresh points per `draw_seed`)."""
     from pacmap_b200 import datasets
 
-    x, _ = datasets.anisotropic_mixture(n=n, d=d, k=50, seed=seed, draw_seed=draw_seed)
+    if generator == "subspace":
+        x, _ = datasets.subspace_mixture(n=n, d=d, k=200, seed=seed, draw_seed=draw_seed)
+    else:
+        x, _ = datasets.anisotropic_mixture(n=n, d=d, k=50, seed=seed, draw_seed=draw_seed)
     return x
 
 
@@ -102,7 +117,7 @@ def config_for(pm, seed):
     return pm.Configuration(initialization=pm.Initialization.Random(7 + seed), seed=7 + seed)
 
 
-def cpu_baseline(n_full, d, sample_n=12000, threads=None):
+def cpu_baseline(n_full, d, sample_n=12000, threads=None, dim=2, generator="anisotropic"):
     """Time the oracle (C++/OpenMP restatement of the reference) on a sample and project to n_full.
 
     The exact kNN is O(n^2 d) and is scaled by (n_full / sample_n)^2; pair sampling, the CSR-free
@@ -111,7 +126,7 @@ def cpu_baseline(n_full, d, sample_n=12000, threads=None):
     import oracle
 
     cores = oracle.set_threads(threads or os.cpu_count() or 1)
-    x = make_data(sample_n, d, seed=99)
+    x = make_data(sample_n, d, seed=99, generator=generator)
     t0 = time.perf_counter()
     xp, *_ = oracle.preprocess(x)
     t1 = time.perf_counter()
@@ -122,7 +137,7 @@ def cpu_baseline(n_full, d, sample_n=12000, threads=None):
     pnn = oracle.sample_neighbors_pair(oracle.scale_dist(kd, oracle.sigma(kd), ki), ki, k)
     pmn = oracle.sample_mn_pairs(xp, n_mn, 7)
     pfp = oracle.sample_fp_pairs(pnn, sample_n, k, n_fp, 7)
-    y0 = oracle.init_random(sample_n, 2, 7)
+    y0 = oracle.init_random(sample_n, dim, 7)
     t3 = time.perf_counter()
     oracle.optimize(y0, pnn, pmn, pfp)
     t4 = time.perf_counter()
@@ -131,7 +146,7 @@ def cpu_baseline(n_full, d, sample_n=12000, threads=None):
     s = n_full / sample_n
     projected = lin * s + quad * s * s
     return {"value": round(projected, 3), "unit": "s", "cores": cores, "kind": "port",
-            "sample": (f"oracle fit_transform on {sample_n}x{d} of the same generator (k={k}, n_mn={n_mn}, "
+            "sample": (f"oracle fit_transform on {sample_n}x{d} -> {dim}-D of the same generator (k={k}, n_mn={n_mn}, "
                        f"n_fp={n_fp}, 450 iters): kNN {quad:.2f}s scaled x{s * s:.0f}, rest {lin:.2f}s scaled "
                        f"x{s:.0f}; reference Rust crate unavailable (no cargo in the image)"),
             "measured_s": round(t4 - t0, 3)}
@@ -140,15 +155,16 @@ def cpu_baseline(n_full, d, sample_n=12000, threads=None):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    base = cpu_baseline(args.n, args.d)
+    w = WORKLOADS[args.workload]
+    base = cpu_baseline(args.n, args.d, dim=w["dim"], generator=w["generator"])
     steps = []
     for _ in range(args.steps):
         steps.append(base["value"])
     v = float(np.mean(steps))
-    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+    line = {"metric": w["metric"], "value": v, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": v * 1000, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"plain PaCMAP {args.n}x{args.d} -> 2-D, 450 iterations, exact kNN", "n": args.n,
+            "config": {"workload": f"plain PaCMAP {args.n}x{args.d} -> {w['dim']}-D, 450 iterations, exact kNN", "n": args.n,
                        "d": args.d},
             "cpu_baseline": base, "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -188,17 +204,18 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as tdist
 
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    n, d, dim = args.n, args.d, 2
-    n_train = min(200_000, max(n // 5, 4096))
+    w = WORKLOADS[args.workload]
+    n, d, dim, gen = args.n, args.d, w["dim"], w["generator"]
+    n_train = min(w["n_train"], max(n // 5, 4096))
     # the learned initialiser is trained once per generator (outside the timed region): plain GPU PaCMAP
     # of n_train draws, then AdamW on (x', embedding)
     train_s, train_losses = None, None
     if args.minimal:
         params = learned.init_params(d, dim, seed=0)
     else:
-        x_train = make_data(n_train, d, seed=0, draw_seed=10_000 + rank)
+        x_train = make_data(n_train, d, seed=0, draw_seed=10_000 + rank, generator=gen)
         y_train, _ = pm.fit_transform(x_train, pm.Configuration(initialization=pm.Initialization.Random(7), seed=7,
-                                                                device=local_rank))
+                                                                embedding_dimensions=dim, device=local_rank))
         xp_train, *_ = pm.stages.preprocess(x_train, local_rank)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -207,9 +224,11 @@ def run_ours(args, rank, world, local_rank):
         train_s = time.perf_counter() - t0
         del x_train, y_train, xp_train
     # a fresh draw of the same generator
-    x = make_data(n, d, seed=0, draw_seed=1000 + rank)
-    cfg_plain = pm.Configuration(initialization=pm.Initialization.Random(7), seed=7, device=local_rank)
-    cfg_short = pm.Configuration(seed=7, num_iters=learned.SHORT_SCHEDULE, device=local_rank)
+    x = make_data(n, d, seed=0, draw_seed=1000 + rank, generator=gen)
+    cfg_plain = pm.Configuration(initialization=pm.Initialization.Random(7), seed=7, embedding_dimensions=dim,
+                                 device=local_rank)
+    cfg_short = pm.Configuration(seed=7, num_iters=learned.SHORT_SCHEDULE, embedding_dimensions=dim,
+                                 device=local_rank)
     dev = f"cuda:{local_rank}"
     dx = torch.from_numpy(x).to(dev)
     dy_l = torch.empty((n, dim), dtype=torch.float32, device=dev)
@@ -225,7 +244,7 @@ def run_ours(args, rank, world, local_rank):
             # the run missed the plain run's 10-NN preservation by more than 0.005: continue it on the
             # plain schedule from where it stopped
             cont = pm.Configuration(initialization=pm.Initialization.Value(dy_l.cpu().numpy()), seed=7,
-                                    device=local_rank)
+                                    embedding_dimensions=dim, device=local_rank)
             pm.fit_transform_device(dx.data_ptr(), n, d, dy_c.data_ptr(), cont)
 
     def step_plain():
@@ -315,13 +334,13 @@ def run_ours(args, rank, world, local_rank):
     opt_gbs = opt_bytes / (opt_ms * 1e-3) / 1e9 if opt_ms > 0 else None
     rnd = lambda q: {"knn10_preservation": round(q[0], 5), "triplet_accuracy": round(q[1], 4)}  # noqa: E731
     line = {
-        "metric": METRIC, "value": round(per_step / 1000.0 / world, 4), "unit": "s", "n_gpus": world,
+        "metric": w["metric"], "value": round(per_step / 1000.0 / world, 4), "unit": "s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": (f"learned-init PaCMAP of a fresh {n}x{d} draw -> 2-D: MLP {d}-512-512-2 prediction "
-                                f"as Value init + schedule {learned.SHORT_SCHEDULE}; vs plain Random(7) with "
-                                f"{learned.PLAIN_SCHEDULE}; exact kNN (k'={min(40 + 50, n - 1)})"),
-                   "n": n, "d": d, "generator": "anisotropic 50-Gaussian mixture (seed 0; draw seed 1000+rank)",
+        "config": {"workload": (f"learned-init PaCMAP of a fresh {n}x{d} draw -> {dim}-D: MLP {d}-512-512-{dim} "
+                                f"prediction as Value init + schedule {learned.SHORT_SCHEDULE}; vs plain Random(7) "
+                                f"with {learned.PLAIN_SCHEDULE}; exact kNN (k'={min(_pair_counts(n)[0] + 50, n - 1)})"),
+                   "n": n, "d": d, "dim": dim, "generator": w["generator_desc"],
                    "mlp_training": f"{n_train} draws (draw seed 10000+rank), plain GPU embedding, 20 epochs, batch "
                                    "4096, AdamW lr 1e-3 wd 1e-4 (outside the timed region)",
                    "l2": "inputs larger than L2 (x = %.0f MB)" % (n * d * 4 / 1e6), "parallelism": f"replicas{world}",
@@ -350,7 +369,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(n, d)
+        line["cpu_baseline"] = cpu_baseline(n, d, dim=dim, generator=gen)
     print(json.dumps(line), flush=True)
     if dist:
         tdist.destroy_process_group()
@@ -362,12 +381,17 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=1_000_000)
-    ap.add_argument("--d", type=int, default=128)
+    ap.add_argument("--workload", default="1m-128", choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=None, help="rows (default: the workload's)")
+    ap.add_argument("--d", type=int, default=None, help="columns (default: the workload's)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--minimal", action="store_true",
                     help="profiling runs: only warm-up + timed steps (no stage timing, e2e or quality passes)")
     args = ap.parse_args()
+    if args.n is None:
+        args.n = WORKLOADS[args.workload]["n"]
+    if args.d is None:
+        args.d = WORKLOADS[args.workload]["d"]
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus else 1)))
     if "RANK" not in os.environ:

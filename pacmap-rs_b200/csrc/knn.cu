@@ -9,7 +9,9 @@
 //   * knn_simt_kernel: every distance in the reference's exact f32 order (distance.rs:50-75) on CUDA
 //     cores, each block keeping the running k' best (distance key, index) of 32 query rows in shared
 //     memory. Used for small n, for any d, and as the fallback for rows the tensor-core filter
-//     (knn_tc.cu) cannot settle.
+//     (knn_tc.cu) cannot settle. When there are too few query rows to fill the GPU, the keys are split
+//     into slices (grid y); each slice writes its own k' best per row and knn_merge_kernel merges
+//     them (the keys are totally ordered, so the merged lists are the same).
 #include "engine.cuh"
 #include "knn_tc.cuh"
 
@@ -26,7 +28,8 @@ constexpr int SQ_MAX_K = 448;     // P = next_pow2(K + KT) <= 512
 __global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __restrict__ x, uint64_t n, int d, int K,
                                                               int P, const uint32_t* __restrict__ rows,
                                                               uint64_t n_rows, uint32_t* __restrict__ out_idx,
-                                                              float* __restrict__ out_dist, int scatter) {
+                                                              float* __restrict__ out_dist, int scatter,
+                                                              uint64_t slice, uint64_t* __restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* qs = reinterpret_cast<float*>(smem);
   float* ks = qs + SQ_QB * SQ_LD;
@@ -50,7 +53,10 @@ __global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __res
   __syncthreads();
 
   const int nc8 = (d / 8) * 8;  // the lane-accumulated part; the tail d % 8 is added after the lane sum
-  for (uint64_t key0 = 0; key0 < n; key0 += SQ_KT) {
+  // keys [kbeg, kend) of this block's slice (slice is a multiple of SQ_KT)
+  const uint64_t kbeg = static_cast<uint64_t>(blockIdx.y) * slice;
+  const uint64_t kend = kbeg + slice < n ? kbeg + slice : n;
+  for (uint64_t key0 = kbeg; key0 < kend; key0 += SQ_KT) {
     float acc[8][8];
 #pragma unroll
     for (int q = 0; q < 8; ++q)
@@ -68,7 +74,7 @@ __global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __res
       for (int e = tid; e < SQ_KT * dlen; e += SQ_THREADS) {
         const int kk = e / dlen, cc = e - kk * dlen;
         const uint64_t j = key0 + kk;
-        ks[kk * SQ_LD + cc] = (j < n) ? x[j * d + dbase + cc] : 0.0f;
+        ks[kk * SQ_LD + cc] = (j < kend) ? x[j * d + dbase + cc] : 0.0f;
       }
       __syncthreads();
       for (int c8 = 0; c8 < dlen; c8 += 8) {
@@ -98,7 +104,7 @@ __global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __res
       float t = 0.0f;
 #pragma unroll
       for (int l = 0; l < 8; ++l) t = __fadd_rn(t, acc[q][l]);
-      if (r == ~0ull || j >= n || j == r) continue;
+      if (r == ~0ull || j >= kend || j == r) continue;
       for (int e = nc8; e < d; ++e) {
         const float df = __fsub_rn(x[r * d + e], x[j * d + e]);
         t = __fadd_rn(t, __fmul_rn(df, df));
@@ -133,9 +139,42 @@ __global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __res
     const uint64_t s = slot0 + qi;
     if (s >= n_rows) continue;
     const uint64_t key = lists[qi * P + cc];
+    if (part) {  // one slice of several: its sorted k' best, merged by knn_merge_kernel
+      part[(s * gridDim.y + blockIdx.y) * K + cc] = key;
+      continue;
+    }
     const uint64_t o = scatter ? qrow[qi] : s;
     out_idx[o * K + cc] = static_cast<uint32_t>(key & 0xFFFFFFFFu);
     out_dist[o * K + cc] = key_to_float(static_cast<uint32_t>(key >> 32));
+  }
+}
+
+// One warp per query row: merges the rows' `slices` sorted lists of K keys into the K smallest, by
+// repeated bitonic sorts of (running K best + next slice) in shared memory.
+constexpr int MG_WARPS = 4;
+__global__ void __launch_bounds__(MG_WARPS * 32) knn_merge_kernel(const uint64_t* __restrict__ part, int slices,
+                                                                   int K, int P2, const uint32_t* __restrict__ rows,
+                                                                   uint64_t n_rows, uint32_t* __restrict__ out_idx,
+                                                                   float* __restrict__ out_dist, int scatter) {
+  extern __shared__ __align__(16) unsigned char msmem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t* buf = reinterpret_cast<uint64_t*>(msmem) + static_cast<size_t>(warp) * P2;
+  const uint64_t s = static_cast<uint64_t>(blockIdx.x) * MG_WARPS + warp;
+  if (s >= n_rows) return;
+  const uint64_t* src = part + s * static_cast<uint64_t>(slices) * K;
+  for (int e = lane; e < K; e += 32) buf[e] = src[e];
+  for (int q = 1; q < slices; ++q) {
+    __syncwarp();
+    for (int e = lane; e < K; e += 32) buf[K + e] = src[static_cast<uint64_t>(q) * K + e];
+    for (int e = 2 * K + lane; e < P2; e += 32) buf[e] = ~0ull;
+    warp_bitonic_sort_u64(buf, P2);
+  }
+  __syncwarp();
+  const uint64_t o = scatter ? static_cast<uint64_t>(rows[s]) : s;
+  for (int e = lane; e < K; e += 32) {
+    const uint64_t key = buf[e];
+    out_idx[o * K + e] = static_cast<uint32_t>(key & 0xFFFFFFFFu);
+    out_dist[o * K + e] = key_to_float(static_cast<uint32_t>(key >> 32));
   }
 }
 
@@ -151,9 +190,33 @@ void knn_rows_simt(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   const int P = next_pow2(K + SQ_KT);
   const size_t smem = static_cast<size_t>(SQ_QB + SQ_KT) * SQ_LD * sizeof(float) + static_cast<size_t>(SQ_QB) * P * 8;
   PM_CUDA(cudaFuncSetAttribute(knn_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  knn_simt_kernel<<<ceil_div(n_rows, SQ_QB), SQ_THREADS, smem, c.stream>>>(d_x, n, static_cast<int>(d), K, P, d_rows,
-                                                                         n_rows, d_idx, d_dist, scatter ? 1 : 0);
+  // Key slices: enough blocks for two waves when the query rows alone do not fill the GPU; every slice
+  // keeps at least 4096 keys (a multiple of the key tile).
+  int per_sm = 1;
+  PM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_simt_kernel, SQ_THREADS, smem));
+  const uint64_t row_blocks = ceil_div(n_rows, SQ_QB);
+  const uint64_t want = 2ull * c.sm_count * static_cast<uint64_t>(std::max(per_sm, 1));
+  uint64_t slices = std::min<uint64_t>((want + row_blocks - 1) / row_blocks, std::max<uint64_t>(n / 4096, 1));
+  slices = std::min<uint64_t>(slices, 1024);
+  slices = std::max<uint64_t>(slices, 1);
+  uint64_t slice = (n + slices - 1) / slices;
+  slice = (slice + SQ_KT - 1) / SQ_KT * SQ_KT;
+  slices = (n + slice - 1) / slice;
+  DevBuf<uint64_t> part;
+  if (slices > 1) part.alloc(c, n_rows * slices * static_cast<uint64_t>(K));
+  const dim3 grid(static_cast<unsigned>(row_blocks), static_cast<unsigned>(slices));
+  knn_simt_kernel<<<grid, SQ_THREADS, smem, c.stream>>>(d_x, n, static_cast<int>(d), K, P, d_rows, n_rows, d_idx,
+                                                         d_dist, scatter ? 1 : 0, slice,
+                                                         slices > 1 ? part.get() : nullptr);
   PM_LAUNCHED();
+  if (slices > 1) {
+    const int P2 = next_pow2(2 * K);
+    const size_t msm = static_cast<size_t>(MG_WARPS) * P2 * sizeof(uint64_t);
+    PM_CUDA(cudaFuncSetAttribute(knn_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm)));
+    knn_merge_kernel<<<ceil_div(n_rows, MG_WARPS), MG_WARPS * 32, msm, c.stream>>>(
+        part.get(), static_cast<int>(slices), K, P2, d_rows, n_rows, d_idx, d_dist, scatter ? 1 : 0);
+    PM_LAUNCHED();
+  }
 }
 
 void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, int mode, uint32_t* d_idx,

@@ -72,17 +72,19 @@ def anisotropic_mixture(n=1_000_000, d=128, k=50, seed=0, chunk=1 << 16, draw_se
     return x[perm], labels[perm]
 
 
-def subspace_mixture(n=4_000_000, d=256, k=200, sub=32, noise=0.05, seed=0, chunk=1 << 16):
+def subspace_mixture(n=4_000_000, d=256, k=200, sub=32, noise=0.05, seed=0, chunk=1 << 16, draw_seed=None):
+    """``seed`` fixes the subspace and the centres; ``draw_seed`` (default: the same stream) the points."""
     rng = np.random.default_rng(seed)
+    rd = rng if draw_seed is None else np.random.default_rng(draw_seed)
     basis = _rotation(rng, d)
     on, off = basis[:, :sub], basis[:, sub:]
     centres = rng.normal(0.0, 4.0, size=(k, sub))
-    labels = rng.integers(0, k, size=n).astype(np.int32)
+    labels = rd.integers(0, k, size=n).astype(np.int32)
     x = np.empty((n, d), np.float32)
     for s in range(0, n, chunk):
         e = min(n, s + chunk)
-        z = centres[labels[s:e]] + rng.normal(size=(e - s, sub))
-        w = noise * rng.normal(size=(e - s, d - sub))
+        z = centres[labels[s:e]] + rd.normal(size=(e - s, sub))
+        w = noise * rd.normal(size=(e - s, d - sub))
         x[s:e] = (z @ on.T + w @ off.T).astype(np.float32)
     return x, labels
 

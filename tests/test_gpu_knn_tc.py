@@ -91,3 +91,20 @@ def test_tc_knn_subspace_mixture_slice_256(lib):
     x, _ = datasets.subspace_mixture(n=100000, d=256, seed=2)
     xp = lib.stages.preprocess(x)[0]
     _tc_vs_simt(lib, xp, 99)
+
+
+def test_simt_knn_key_slices(lib, orc):
+    # 9,000 rows on the exact SIMT path: the keys are split into two slices whose lists are merged
+    x = _mix(9000, 16, seed=4)
+    gi, gd = lib.knn.find_k_nearest_neighbors(x, 30, knn_mode=3)
+    ei, ed = orc.knn_exact(x, 30)
+    assert np.array_equal(gd, ed) and np.array_equal(gi, ei)
+
+
+def test_tc_knn_fallback_rows_over_key_slices(lib, orc):
+    # 700 duplicates overflow the filter's buffers; those few rows are recomputed over ~9 key slices
+    x = _mix(40000, 24, seed=8)
+    x[1000:1700] = x[5]
+    gi, gd = lib.knn.find_k_nearest_neighbors(x, 60, knn_mode=F16)
+    ei, ed = orc.knn_exact(x, 60)
+    assert np.array_equal(gd, ed) and np.array_equal(gi, ei)
