@@ -277,7 +277,7 @@ __global__ void sample_mn_kernel(const float* __restrict__ x, uint64_t n, int d,
 // sample_mn_kernel with the picks (n_mn <= 32) in one register per lane and row i of x (d <= 8 NC)
 // in NC registers of each 8-lane group.
 template <int NC>
-__global__ void sample_mn_reg_kernel(const float* __restrict__ x, uint64_t n, int d, uint32_t n_mn, uint64_t seed,
+__global__ void __launch_bounds__(256, NC <= 16 ? 4 : 3) sample_mn_reg_kernel(const float* __restrict__ x, uint64_t n, int d, uint32_t n_mn, uint64_t seed,
                                      uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
   const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
   const uint32_t lane = lane_id();
@@ -321,6 +321,20 @@ __global__ void sample_mn_reg_kernel(const float* __restrict__ x, uint64_t n, in
       if (failed) {
         if (lane == 0) atomicOr(err, DEV_ERR_SAMPLING);
         break;
+      }
+      // The candidates' rows are random HBM reads: start all of them towards L2 now (one 128-byte line
+      // per lane and step), so the second pass below finds its rows there.
+      {
+        const int lines = (d * 4 + 127) / 128;
+        for (int q = static_cast<int>(lane); q < static_cast<int>(cnt) * lines; q += 32) {
+          const int slot = q / lines, ln = q - slot * lines;
+          uint32_t cj = 0;
+#pragma unroll
+          for (int t = 0; t < 6; ++t)
+            if (t == slot) cj = cand[t];
+          const char* line = reinterpret_cast<const char*>(x + static_cast<uint64_t>(cj) * d) + ln * 128;
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+        }
       }
       // Distances of the drawn candidates in the reference's order (group8_ref_dist with row i in
       // registers): group g (lanes 8g..8g+7) handles slots g and g + 4.
