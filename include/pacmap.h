@@ -45,6 +45,7 @@ typedef enum pacmap_status {
   PACMAP_ERR_PAIR_INDEX = 21,               /* a provided pair names a point >= n (the ref. panics)  */
   PACMAP_ERR_SAMPLING = 22,                 /* distinct partners cannot be drawn (the ref. spins)    */
   PACMAP_ERR_UNSUPPORTED = 23,              /* Initialization::Pca, or a size beyond a kernel limit  */
+  PACMAP_ERR_MODEL_FILE = 24,               /* a model file cannot be read/written or is damaged     */
   PACMAP_ERR_CUDA = 30,                     /* CUDA runtime error (message has the detail)           */
   PACMAP_ERR_OOM = 31,                      /* device allocation failed                              */
   PACMAP_ERR_NO_DEVICE = 32,                /* no CUDA device of compute capability 10.x             */
@@ -206,6 +207,31 @@ pacmap_status pacmap_fit_transform_learned(const float* x, uint64_t n, uint64_t 
 pacmap_status pacmap_fit_transform_learned_device(const float* d_x, uint64_t n, uint64_t d, const pacmap_config* cfg,
                                                   const float* mlp_params, float* d_out_embedding,
                                                   float* d_out_snapshots);
+
+/* --- the learned model on disk and the transform of new points (no reference analogue: the reference
+ * embeds only the points it was fitted on, README.md:165) ---
+ * A model is the MLP above, its training data's preprocessing constants (pacmap_preprocess's min, max
+ * and column means) and the per-dimension mean and standard deviation of the training embedding (the
+ * network predicts z-scored coordinates). */
+/* out_mean, out_std (dim values each) of an embedding y (n x dim): the standardisation that
+ * pacmap_mlp_train applies to its targets. */
+pacmap_status pacmap_model_target_stats(const float* y, uint64_t n, uint64_t dim, float* out_mean, float* out_std);
+/* Writes a model file (format in pacmap-rs_b200/csrc/model.cu; checksummed). params: the flat layout
+ * of pacmap_mlp_param_count(d, dim) values; pre_mean: d values; target_mean, target_std: dim values. */
+pacmap_status pacmap_model_save(const char* path, uint64_t d, uint64_t dim, const float* params, float pre_min,
+                                float pre_max, const float* pre_mean, const float* target_mean,
+                                const float* target_std);
+/* Reads a model file; every output may be NULL (read out_d and out_dim first, then size the buffers).
+ * A damaged, truncated or foreign file returns PACMAP_ERR_MODEL_FILE. */
+pacmap_status pacmap_model_load(const char* path, uint64_t* out_d, uint64_t* out_dim, float* out_params,
+                                float* out_pre_min, float* out_pre_max, float* out_pre_mean,
+                                float* out_target_mean, float* out_target_std);
+/* Embeds new points x (n x d, raw data like the training data) into the training embedding's
+ * coordinates: x' = (x - pre_min) / pre_max - pre_mean (preprocess_x's f32 arithmetic with the stored
+ * constants), then out (n x dim) = MLP(x') * target_std + target_mean. */
+pacmap_status pacmap_transform(const float* x, uint64_t n, uint64_t d, uint64_t dim, const float* params,
+                               float pre_min, float pre_max, const float* pre_mean, const float* target_mean,
+                               const float* target_std, int32_t device, float* out_embedding);
 
 /* Quality of an embedding (no reference analogue): mean 10-NN preservation over `sample` (n_sample
  * point indices; neighbours by the reference's f32 distance on the preprocessed data) and random-triplet

@@ -139,12 +139,6 @@ uint64_t entropy_seed() {
   return (static_cast<uint64_t>(rd()) << 32) ^ rd();
 }
 
-template <typename T>
-void upload(Ctx& c, DevBuf<T>& dst, const T* src, size_t count) {
-  dst.alloc(c, count);
-  if (count) PM_CUDA(cudaMemcpyAsync(dst.get(), src, count * sizeof(T), cudaMemcpyHostToDevice, c.stream));
-}
-
 // Device-time marks between the stages of one call (CUDA events on the call's stream).
 enum Stage { ST_PRE = 0, ST_KNN, ST_RESELECT, ST_MN, ST_FP, ST_CSR, ST_INIT, ST_OPT, ST_COUNT };
 struct StageTimer {
@@ -485,6 +479,50 @@ pacmap_status pacmap_mlp_apply(const float* params, uint64_t d, uint64_t dim, co
     upload(c, dx, xp, n * d);
     mlp_apply_device(c, params, d, dim, dx.get(), n, dy.get());
     PM_CUDA(cudaMemcpyAsync(out, dy.get(), dy.bytes(), cudaMemcpyDeviceToHost, c.stream));
+    PM_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+pacmap_status pacmap_model_target_stats(const float* y, uint64_t n, uint64_t dim, float* out_mean, float* out_std) {
+  return guarded([&] {
+    PM_REQUIRE(y && out_mean && out_std, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    PM_REQUIRE(n > 0, PACMAP_ERR_EMPTY_ARRAY_MEAN, "Failed to calculate mean axis: the array is empty");
+    model_target_stats(y, n, dim, out_mean, out_std);
+  });
+}
+
+pacmap_status pacmap_model_save(const char* path, uint64_t d, uint64_t dim, const float* params, float pre_min,
+                                float pre_max, const float* pre_mean, const float* target_mean,
+                                const float* target_std) {
+  return guarded([&] {
+    PM_REQUIRE(path && params && pre_mean && target_mean && target_std, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    model_save(path, d, dim, params, pre_min, pre_max, pre_mean, target_mean, target_std);
+  });
+}
+
+pacmap_status pacmap_model_load(const char* path, uint64_t* out_d, uint64_t* out_dim, float* out_params,
+                                float* out_pre_min, float* out_pre_max, float* out_pre_mean,
+                                float* out_target_mean, float* out_target_std) {
+  return guarded([&] {
+    PM_REQUIRE(path != nullptr, PACMAP_ERR_INVALID_ARGUMENT, "NULL path");
+    model_load(path, out_d, out_dim, out_params, out_pre_min, out_pre_max, out_pre_mean, out_target_mean,
+               out_target_std);
+  });
+}
+
+pacmap_status pacmap_transform(const float* x, uint64_t n, uint64_t d, uint64_t dim, const float* params,
+                               float pre_min, float pre_max, const float* pre_mean, const float* target_mean,
+                               const float* target_std, int32_t device, float* out_embedding) {
+  return guarded([&] {
+    PM_REQUIRE(params && pre_mean && target_mean && target_std && (n == 0 || (x && out_embedding)),
+               PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (n == 0) return;
+    DeviceLock dl(device);
+    Ctx& c = dl.ctx;
+    DevBuf<float> dx, dy(c, n * dim);
+    upload(c, dx, x, n * d);
+    transform_device(c, dx.get(), n, d, dim, params, pre_min, pre_max, pre_mean, target_mean, target_std, dy.get());
+    PM_CUDA(cudaMemcpyAsync(out_embedding, dy.get(), dy.bytes(), cudaMemcpyDeviceToHost, c.stream));
     PM_CUDA(cudaStreamSynchronize(c.stream));
   });
 }

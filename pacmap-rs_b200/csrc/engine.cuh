@@ -54,6 +54,13 @@ struct DevBuf {
   size_t bytes() const { return count * sizeof(T); }
 };
 
+// dst = a device copy of count host values (stream-ordered).
+template <typename T>
+void upload(Ctx& c, DevBuf<T>& dst, const T* src, size_t count) {
+  dst.alloc(c, count);
+  if (count) PM_CUDA(cudaMemcpyAsync(dst.get(), src, count * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+}
+
 // ---- preprocess.cu ----
 // preprocess_x non-PCA branch on the device; h_min/h_max receive the total-order extrema.
 void preprocess_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float* d_out, float* h_min, float* h_max,

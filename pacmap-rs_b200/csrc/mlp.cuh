@@ -14,4 +14,17 @@ void mlp_grad_device(Ctx& c, const float* params, uint64_t d, uint64_t dim, cons
 // AdamW training on (x, t) rows (device), params updated in place (host flat layout).
 void mlp_train_device(Ctx& c, float* params, uint64_t d, uint64_t dim, const float* d_x, const float* d_t, uint64_t n,
                       uint64_t epochs, uint64_t batch, float lr, float wd, uint64_t seed, float* epoch_loss);
+
+// ---- model.cu: the learned model on disk and the transform of new points ----
+// Per-dimension mean and population std of an embedding (the standardisation of the MLP's targets).
+void model_target_stats(const float* y, uint64_t n, uint64_t dim, float* mean, float* sd);
+void model_save(const char* path, uint64_t d, uint64_t dim, const float* params, float pre_min, float pre_max,
+                const float* pre_mean, const float* t_mean, const float* t_std);
+// Any output pointer may be NULL (query the shape first, then read with buffers of that size).
+void model_load(const char* path, uint64_t* d, uint64_t* dim, float* params, float* pre_min, float* pre_max,
+                float* pre_mean, float* t_mean, float* t_std);
+// out (n x dim, device) = MLP((x - min) / max - mean) * std + mean_t for device x (n x d); host constants.
+void transform_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t dim, const float* params,
+                      float pre_min, float pre_max, const float* pre_mean, const float* t_mean, const float* t_std,
+                      float* d_out);
 }  // namespace pacmap

@@ -66,6 +66,7 @@ _ERRORS = {
     21: _variant("PairIndexOutOfRange", 21, "A provided pair names a point >= n (the reference panics)."),
     22: _variant("SamplingFailed", 22, "Distinct partners cannot be drawn (the reference loops forever)."),
     23: _variant("Unsupported", 23, "Initialization::Pca, or a size beyond a kernel limit."),
+    24: _variant("ModelFileError", 24, "A model file cannot be read or written, or is damaged."),
     30: _variant("CudaError", 30, "CUDA runtime error."),
     31: _variant("OutOfMemory", 31, "Device allocation failed."),
     32: _variant("NoDevice", 32, "No CUDA device of compute capability 10.x."),

@@ -6,6 +6,10 @@ the (x, embedding) pairs that a plain fit produces for one data generator, and s
 same generator from its prediction, so that a shortened schedule (``SHORT_SCHEDULE``) replaces the
 plain one (``PLAIN_SCHEDULE``). Training, inference and the gradient check all run on the GPU
 (tcgen05 BF16 GEMMs with FP32 accumulation, AdamW) through the C ABI (include/pacmap.h).
+
+``LearnedModel`` bundles a trained network with its training data's preprocessing constants and the
+training embedding's scale: it is saved to and loaded from a file, and ``transform`` embeds points the
+fit never saw into that embedding's coordinates (the reference cannot, README.md:165).
 """
 from __future__ import annotations
 
@@ -15,7 +19,7 @@ from typing import Optional
 
 import numpy as np
 
-from . import Configuration, Initialization, _abi, _check, _CConfig
+from . import Configuration, Initialization, _abi, _check, _CConfig, stages
 from ._abi import ptr
 
 PLAIN_SCHEDULE = (100, 100, 250)
@@ -101,3 +105,80 @@ def fit_transform_learned_device(x_ptr: int, n: int, d: int, out_ptr: int, param
     _check(_abi.lib().pacmap_fit_transform_learned_device(C.c_void_p(x_ptr), n, d, C.byref(cc.c), ptr(p),
                                                           C.c_void_p(out_ptr),
                                                           C.c_void_p(snapshots_ptr) if snapshots_ptr else None))
+
+
+@dataclasses.dataclass
+class LearnedModel:
+    """A trained initialiser plus what ``transform`` needs: ``params`` (flat MLP layout), the training
+    data's preprocessing constants (``pre_min``, ``pre_max``, ``pre_mean``: preprocess_x's min, max and
+    column means) and the training embedding's per-dimension ``target_mean`` / ``target_std``."""
+
+    params: np.ndarray
+    d: int
+    dim: int
+    pre_min: float
+    pre_max: float
+    pre_mean: np.ndarray
+    target_mean: np.ndarray
+    target_std: np.ndarray
+
+    def save(self, path: str) -> None:
+        _check(_abi.lib().pacmap_model_save(str(path).encode(), self.d, self.dim, ptr(_f32(self.params)),
+                                            float(self.pre_min), float(self.pre_max), ptr(_f32(self.pre_mean)),
+                                            ptr(_f32(self.target_mean)), ptr(_f32(self.target_std))))
+
+    @classmethod
+    def load(cls, path: str) -> "LearnedModel":
+        L = _abi.lib()
+        d, dim = C.c_uint64(0), C.c_uint64(0)
+        _check(L.pacmap_model_load(str(path).encode(), C.byref(d), C.byref(dim), None, None, None, None, None, None))
+        d, dim = int(d.value), int(dim.value)
+        params = np.zeros(param_count(d, dim), np.float32)
+        pre_mean = np.zeros(d, np.float32)
+        t_mean, t_std = np.zeros(dim, np.float32), np.zeros(dim, np.float32)
+        mn, mx = C.c_float(0), C.c_float(0)
+        _check(L.pacmap_model_load(str(path).encode(), None, None, ptr(params), C.byref(mn), C.byref(mx),
+                                   ptr(pre_mean), ptr(t_mean), ptr(t_std)))
+        return cls(params, d, dim, mn.value, mx.value, pre_mean, t_mean, t_std)
+
+    def transform(self, x, device: int = 0) -> np.ndarray:
+        """Embeds new points (raw data like the training data) into the training embedding's coordinates."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        n, d = x.shape
+        assert d == self.d, f"the model expects {self.d} columns, got {d}"
+        out = np.zeros((n, self.dim), np.float32)
+        _check(_abi.lib().pacmap_transform(ptr(x), n, d, self.dim, ptr(_f32(self.params)), float(self.pre_min),
+                                           float(self.pre_max), ptr(_f32(self.pre_mean)),
+                                           ptr(_f32(self.target_mean)), ptr(_f32(self.target_std)), device,
+                                           ptr(out)))
+        return out
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def target_stats(y):
+    """Per-dimension (mean, population std) of an embedding: the standardisation of the MLP's targets."""
+    y = _f32(y)
+    n, dim = y.shape
+    mean, std = np.zeros(dim, np.float32), np.zeros(dim, np.float32)
+    _check(_abi.lib().pacmap_model_target_stats(ptr(y), n, dim, ptr(mean), ptr(std)))
+    return mean, std
+
+
+def fit_model(x, embedding, epochs: int = 20, batch: int = 4096, lr: float = 1e-3, weight_decay: float = 1e-4,
+              seed: int = 0, device: int = 0):
+    """Trains a ``LearnedModel`` on raw data x and its embedding (e.g. the plain fit of x).
+
+    Returns (model, loss of each epoch)."""
+    x = _f32(x)
+    y = _f32(embedding)
+    n, d = x.shape
+    dim = y.shape[1]
+    xp, mn, mx, mean = stages.preprocess(x, device)
+    batch = min(batch, n // 128 * 128)
+    params, losses = train(init_params(d, dim, seed), xp, y, epochs=epochs, batch=batch, lr=lr,
+                           weight_decay=weight_decay, seed=seed, device=device)
+    t_mean, t_std = target_stats(y)
+    return LearnedModel(params, d, dim, float(mn), float(mx), _f32(mean), t_mean, t_std), losses
