@@ -44,7 +44,7 @@ typedef enum pacmap_status {
   PACMAP_ERR_INVALID_ARGUMENT = 20,         /* NULL pointer / bad enum / size overflow               */
   PACMAP_ERR_PAIR_INDEX = 21,               /* a provided pair names a point >= n (the ref. panics)  */
   PACMAP_ERR_SAMPLING = 22,                 /* distinct partners cannot be drawn (the ref. spins)    */
-  PACMAP_ERR_UNSUPPORTED = 23,              /* Initialization::Pca, or a size beyond a kernel limit  */
+  PACMAP_ERR_UNSUPPORTED = 23,              /* a size beyond a kernel limit                          */
   PACMAP_ERR_MODEL_FILE = 24,               /* a model file cannot be read/written or is damaged     */
   PACMAP_ERR_CUDA = 30,                     /* CUDA runtime error (message has the detail)           */
   PACMAP_ERR_OOM = 31,                      /* device allocation failed                              */
@@ -52,7 +52,9 @@ typedef enum pacmap_status {
   PACMAP_ERR_DEVICE_INVARIANT = 33          /* a kernel's own check failed (index range, timeout)    */
 } pacmap_status;
 
-/* Initialization (src/lib.rs:226-239). PCA is not built: PACMAP_ERR_UNSUPPORTED. */
+/* Initialization (src/lib.rs:226-239). PCA: the exact principal axes (pacmap-rs_b200/csrc/pca.cu) where
+ * the reference calls petal-decomposition's SVD / randomized SVD; with d > 100 the pairs are drawn on
+ * the projection onto min(100, n) axes, as the reference does (src/lib.rs:455-480). */
 typedef enum pacmap_init_kind {
   PACMAP_INIT_PCA = 0,
   PACMAP_INIT_VALUE = 1,  /* Value(Array2<f32>): init_value, n x embedding_dimensions           */

@@ -215,20 +215,34 @@ void validate_config(const pacmap_config* cfg) {
   PM_REQUIRE(cfg->knn_mode >= 0 && cfg->knn_mode <= 3, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
 }
 
+// preprocess_x (src/lib.rs:442-522): the normalised data, or -- with Initialization::Pca and more than 100
+// columns (:455) -- the projection onto min(100, n) principal axes, on which the pairs are then drawn
+// (pca_solution). Returns the working data's column count.
+uint64_t preprocess_for(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const pacmap_config& cfg, bool learned,
+                        DevBuf<float>& xp) {
+  if (cfg.init_kind == PACMAP_INIT_PCA && !learned && d > 100) {
+    const uint64_t k = std::min<uint64_t>(100, n);
+    xp.alloc(c, n * k);
+    pca_project_device(c, d_x, n, d, k, 1.0f, xp.get(), nullptr);
+    return k;
+  }
+  xp.alloc(c, n * d);
+  preprocess_device(c, d_x, n, d, xp.get(), nullptr, nullptr, nullptr);
+  return d;
+}
+
 // fit_transform with x already on the device; h_* pointers are the caller's host views of the config.
 void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const pacmap_config& cfg, float* d_out,
                         float* d_snap, const float* mlp_params = nullptr) {
   // lib.rs:300-302
   PM_REQUIRE(n > 1, PACMAP_ERR_SAMPLE_SIZE, "Sample size must be larger than one");
   const uint64_t dim = cfg.embedding_dimensions;
-  PM_REQUIRE(cfg.init_kind != PACMAP_INIT_PCA || mlp_params != nullptr, PACMAP_ERR_UNSUPPORTED,
-             "Initialization::Pca is not built in this engine; use Value or Random");
   PM_REQUIRE(dim <= 8, PACMAP_ERR_UNSUPPORTED, "embedding dimensions above 8 are not supported");
   StageTimer tm(c.stream);
   // lib.rs:442-522 (the PCA branch is never taken: init is Value or Random)
-  DevBuf<float> xp(c, n * d);
+  DevBuf<float> xp;
   tm.start(ST_PRE);
-  preprocess_device(c, d_x, n, d, xp.get(), nullptr, nullptr, nullptr);
+  const uint64_t dw = preprocess_for(c, d_x, n, d, cfg, mlp_params != nullptr, xp);
   tm.stop(ST_PRE);
   // lib.rs:333-338
   const PairCounts pc = decide_num_pairs(n, cfg);
@@ -236,7 +250,7 @@ void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const 
   // lib.rs:629-692 sample_pairs
   DevPairs pairs;
   if (cfg.pair_kind == PACMAP_PAIRS_GENERATE) {
-    generate_pairs_device(c, xp.get(), n, d, pc, seed, cfg.knn_mode, pairs, &tm);
+    generate_pairs_device(c, xp.get(), n, dw, pc, seed, cfg.knn_mode, pairs, &tm);
   } else if (cfg.pair_kind == PACMAP_PAIRS_NEIGHBORS_PROVIDED) {
     const uint64_t expected = n * pc.k;
     if (cfg.pair_neighbors_rows != expected)
@@ -248,7 +262,7 @@ void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const 
     pairs.n_nn = expected;
     pairs.mn.alloc(c, n * pc.n_mn * 2);
     pairs.n_mn = n * pc.n_mn;
-    sample_mn_device(c, xp.get(), n, d, pc.n_mn, seed, pairs.mn.get());
+    sample_mn_device(c, xp.get(), n, dw, pc.n_mn, seed, pairs.mn.get());
     pairs.fp.alloc(c, n * pc.n_fp * 2);
     pairs.n_fp = n * pc.n_fp;
     sample_fp_device(c, pairs.nn.get(), n, pc.k, pc.n_fp, seed, pairs.fp.get());
@@ -272,6 +286,17 @@ void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const 
     DevBuf<float> raw(c, n * dim);
     mlp_apply_device(c, mlp_params, d, dim, xp.get(), n, raw.get());
     init_value_device(c, raw.get(), n, dim, d_out);
+  } else if (cfg.init_kind == PACMAP_INIT_PCA) {
+    if (dw != d) {
+      // YInit::Preprocessed (lib.rs:765): 0.01 * the leading columns of the PCA projection
+      PM_REQUIRE(dim <= dw, PACMAP_ERR_PCA, "PCA: more embedding dimensions than principal components");
+      leading_columns(c, xp.get(), n, dw, dim, 0.01f, d_out);
+    } else {
+      // YInit::DimensionalReduction (lib.rs:766): Pca(min(n, dim)) fitted on x', its transform * 0.01
+      PM_REQUIRE(dim <= d && dim <= n, PACMAP_ERR_PCA,
+                 "PCA: the embedding needs no more dimensions than the data has columns and rows");
+      pca_project_device(c, xp.get(), n, d, dim, 0.01f, d_out, nullptr);
+    }
   } else if (cfg.init_kind == PACMAP_INIT_VALUE) {
     PM_REQUIRE(cfg.init_value != nullptr, PACMAP_ERR_INVALID_ARGUMENT, "init_value is NULL");
     DevBuf<float> v;
@@ -591,11 +616,11 @@ pacmap_status pacmap_generate_pairs(const float* x, uint64_t n, uint64_t d, cons
     if (!out_pnn && !out_pmn && !out_pfp) return;
     DeviceLock dl(cfg->device);
     Ctx& c = dl.ctx;
-    DevBuf<float> dx, xp(c, n * d);
+    DevBuf<float> dx, xp;
     upload(c, dx, x, n * d);
-    preprocess_device(c, dx.get(), n, d, xp.get(), nullptr, nullptr, nullptr);
+    const uint64_t dw = preprocess_for(c, dx.get(), n, d, *cfg, false, xp);
     DevPairs pairs;
-    generate_pairs_device(c, xp.get(), n, d, pc, cfg->has_seed ? cfg->seed : entropy_seed(), cfg->knn_mode, pairs);
+    generate_pairs_device(c, xp.get(), n, dw, pc, cfg->has_seed ? cfg->seed : entropy_seed(), cfg->knn_mode, pairs);
     if (out_pnn) PM_CUDA(cudaMemcpyAsync(out_pnn, pairs.nn.get(), pairs.nn.bytes(), cudaMemcpyDeviceToHost, c.stream));
     if (out_pmn) PM_CUDA(cudaMemcpyAsync(out_pmn, pairs.mn.get(), pairs.mn.bytes(), cudaMemcpyDeviceToHost, c.stream));
     if (out_pfp) PM_CUDA(cudaMemcpyAsync(out_pfp, pairs.fp.get(), pairs.fp.bytes(), cudaMemcpyDeviceToHost, c.stream));

@@ -95,6 +95,14 @@ struct Csr {
 void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const uint32_t* d_pmn, uint64_t n_mn,
                const uint32_t* d_pfp, uint64_t n_fp, Csr& out);
 void init_value_device(Ctx& c, const float* d_v, uint64_t n, uint64_t dim, float* d_y);
+
+// ---- pca.cu: Initialization::Pca ----
+// d_out (n x k) = scale * (x - column mean) V_k with V_k the k leading principal axes of x (n x d);
+// axes_out (optional) receives V_k (d x k, row-major). k <= 128, d <= 1024.
+void pca_project_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t k, float scale, float* d_out,
+                        std::vector<float>* axes_out);
+// d_out (n x k) = scale * x[:, :k] for x (n x w).
+void leading_columns(Ctx& c, const float* d_x, uint64_t n, uint64_t w, uint64_t k, float scale, float* d_out);
 void init_random_device(Ctx& c, uint64_t n, uint64_t dim, uint64_t seed, float* d_y);
 
 struct OptimizeArgs {

@@ -65,7 +65,7 @@ _ERRORS = {
     20: _variant("InvalidArgument", 20, "A NULL pointer, bad enum or size overflow."),
     21: _variant("PairIndexOutOfRange", 21, "A provided pair names a point >= n (the reference panics)."),
     22: _variant("SamplingFailed", 22, "Distinct partners cannot be drawn (the reference loops forever)."),
-    23: _variant("Unsupported", 23, "Initialization::Pca, or a size beyond a kernel limit."),
+    23: _variant("Unsupported", 23, "A size beyond a kernel limit."),
     24: _variant("ModelFileError", 24, "A model file cannot be read or written, or is damaged."),
     30: _variant("CudaError", 30, "CUDA runtime error."),
     31: _variant("OutOfMemory", 31, "Device allocation failed."),

@@ -303,8 +303,8 @@ def test_errors_like_reference(lib):
         lib.fit_transform(x, lib.Configuration(initialization=R, far_pair_ratio=0.0))
     with pytest.raises(lib.InvalidNeighborCount):
         lib.fit_transform(x, lib.Configuration(initialization=R, override_neighbors=0))
-    with pytest.raises(lib.Unsupported):
-        lib.fit_transform(x, lib.Configuration())  # Initialization::Pca
+    with pytest.raises(lib.Pca):  # Initialization::Pca with more embedding dimensions than columns
+        lib.fit_transform(x, lib.Configuration(embedding_dimensions=6))
     bad = np.array([[0, 1], [5, 100]], np.uint32)
     with pytest.raises(lib.PairIndexOutOfRange):
         lib.fit_transform(x, lib.Configuration(initialization=R, pair_configuration=lib.PairConfiguration.
@@ -334,3 +334,46 @@ def test_deterministic(lib):
     a, _ = lib.fit_transform(x, cfg)
     b, _ = lib.fit_transform(x, cfg)
     assert np.array_equal(a, b)
+
+
+# ----------------------------------------------------------------------------------------------------
+# Initialization::Pca (lib.rs:442-522, 753-768): exact principal axes (the reference's petal-decomposition
+# SVD is not in the tree), each axis's largest loading positive; zero iterations return the start.
+# ----------------------------------------------------------------------------------------------------
+def _axes(z, k):
+    zc = z.astype(np.float64) - z.astype(np.float64).mean(0)
+    w, v = np.linalg.eigh(zc.T @ zc)
+    v = v[:, np.argsort(w)[::-1][:k]]
+    v *= np.sign(v[np.abs(v).argmax(0), np.arange(k)])
+    return zc @ v
+
+
+def test_pca_init_small_d_is_the_projection_of_the_normalised_data(lib, orc):
+    x = _mixture(2000, 30, seed=4)
+    y, _ = lib.fit_transform(x, lib.Configuration(num_iters=(0, 0, 0), seed=1))
+    xp, *_ = orc.preprocess(x)
+    want = 0.01 * _axes(xp, 2)
+    assert np.abs(y - want).max() <= 1e-5 * np.abs(want).max()
+
+
+def test_pca_init_wide_data_uses_the_100_axis_projection(lib):
+    x = _mixture(3000, 150, seed=6)
+    y, _ = lib.fit_transform(x, lib.Configuration(num_iters=(0, 0, 0), seed=1))
+    want = 0.01 * _axes(x, 2)  # the raw data's projection, its leading two columns
+    assert np.abs(y - want).max() <= 1e-4 * np.abs(want).max()
+
+
+def test_pca_default_configuration_embeds_like_random_init(lib):
+    """The reference's default configuration (Initialization::Pca) runs end to end, as well as Random."""
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.isotropic_mixture(n=2000, d=100, k=10, seed=0)
+    sample, trip = datasets.quality_sample(2000, 1000, seed=3)
+    y_pca, _ = lib.fit_transform(x, lib.Configuration(seed=42))
+    y_rnd, _ = lib.fit_transform(x, lib.Configuration(seed=42, initialization=lib.Initialization.Random(42)))
+    q_pca, q_rnd = lib.quality(x, y_pca, sample, trip), lib.quality(x, y_rnd, sample, trip)
+    assert q_pca[1] >= q_rnd[1] - 0.03 and q_pca[0] >= q_rnd[0] - 0.05, (q_pca, q_rnd)
+    # wide data: pairs drawn on the 100-axis projection
+    xw = np.concatenate([x, 0.1 * np.random.default_rng(1).normal(size=(2000, 60)).astype(np.float32)], 1)
+    y_w, _ = lib.fit_transform(xw, lib.Configuration(seed=42))
+    assert np.all(np.isfinite(y_w)) and lib.quality(xw, y_w, sample, trip)[1] >= q_rnd[1] - 0.05
