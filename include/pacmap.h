@@ -76,6 +76,15 @@ typedef enum pacmap_knn_mode {
   PACMAP_KNN_SIMT_EXACT = 3    /* every distance in the reference's FP32 order on CUDA cores        */
 } pacmap_knn_mode;
 
+/* The distance the pairs are drawn with (no reference analogue: the reference is Euclidean only,
+ * README.md:164). ANGULAR divides every preprocessed row by its norm (the reference's f32 distance from
+ * the origin; zero rows stay zero), so that Euclidean distances become the angular distance
+ * sqrt(2 - 2 cos) of the preprocessed rows; the kNN, sigma scaling and mid-near choices follow it. */
+typedef enum pacmap_metric {
+  PACMAP_METRIC_EUCLIDEAN = 0,  /* the reference's metric                                            */
+  PACMAP_METRIC_ANGULAR = 1
+} pacmap_metric;
+
 /* Configuration (src/lib.rs:159-224), field by field, plus the engine's switches at the end.
  * Option<T> fields are a has_ flag plus the value. Pointers are host memory and only read. */
 typedef struct pacmap_config {
@@ -106,6 +115,7 @@ typedef struct pacmap_config {
   int32_t knn_mode;                    /* pacmap_knn_mode, default AUTO                              */
   int32_t device;                      /* CUDA device ordinal, default 0                             */
   float* loss_trace;                   /* optional out: the loss (grad[n,0]) of every iteration      */
+  int32_t metric;                      /* pacmap_metric, default EUCLIDEAN                          */
 } pacmap_config;
 
 /* Configuration::default() (src/lib.rs:208-224) plus the engine defaults. */

@@ -213,22 +213,27 @@ void validate_config(const pacmap_config* cfg) {
   PM_REQUIRE(cfg->init_kind >= 0 && cfg->init_kind <= 2, PACMAP_ERR_INVALID_ARGUMENT, "unknown init_kind");
   PM_REQUIRE(cfg->pair_kind >= 0 && cfg->pair_kind <= 2, PACMAP_ERR_INVALID_ARGUMENT, "unknown pair_kind");
   PM_REQUIRE(cfg->knn_mode >= 0 && cfg->knn_mode <= 3, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
+  PM_REQUIRE(cfg->metric == PACMAP_METRIC_EUCLIDEAN || cfg->metric == PACMAP_METRIC_ANGULAR,
+             PACMAP_ERR_INVALID_ARGUMENT, "unknown metric");
 }
 
 // preprocess_x (src/lib.rs:442-522): the normalised data, or -- with Initialization::Pca and more than 100
 // columns (:455) -- the projection onto min(100, n) principal axes, on which the pairs are then drawn
 // (pca_solution). Returns the working data's column count.
+// With the angular metric the working rows are then scaled to unit norm.
 uint64_t preprocess_for(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const pacmap_config& cfg, bool learned,
                         DevBuf<float>& xp) {
+  uint64_t w = d;
   if (cfg.init_kind == PACMAP_INIT_PCA && !learned && d > 100) {
-    const uint64_t k = std::min<uint64_t>(100, n);
-    xp.alloc(c, n * k);
-    pca_project_device(c, d_x, n, d, k, 1.0f, xp.get(), nullptr);
-    return k;
+    w = std::min<uint64_t>(100, n);
+    xp.alloc(c, n * w);
+    pca_project_device(c, d_x, n, d, w, 1.0f, xp.get(), nullptr);
+  } else {
+    xp.alloc(c, n * d);
+    preprocess_device(c, d_x, n, d, xp.get(), nullptr, nullptr, nullptr);
   }
-  xp.alloc(c, n * d);
-  preprocess_device(c, d_x, n, d, xp.get(), nullptr, nullptr, nullptr);
-  return d;
+  if (cfg.metric == PACMAP_METRIC_ANGULAR) normalize_rows_device(c, xp.get(), n, w);
+  return w;
 }
 
 // fit_transform with x already on the device; h_* pointers are the caller's host views of the config.
@@ -388,6 +393,7 @@ pacmap_config pacmap_config_default(void) {
   c.approx_threshold = 8000;
   c.knn_mode = PACMAP_KNN_AUTO;
   c.device = 0;
+  c.metric = PACMAP_METRIC_EUCLIDEAN;
   return c;
 }
 

@@ -96,6 +96,10 @@ void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const u
                const uint32_t* d_pfp, uint64_t n_fp, Csr& out);
 void init_value_device(Ctx& c, const float* d_v, uint64_t n, uint64_t dim, float* d_y);
 
+// Every row divided by its norm (the reference's f32 distance from the origin, distance.rs:50-75 order);
+// zero rows stay zero. In place, n x d.
+void normalize_rows_device(Ctx& c, float* d_x, uint64_t n, uint64_t d);
+
 // ---- pca.cu: Initialization::Pca ----
 // d_out (n x k) = scale * (x - column mean) V_k with V_k the k leading principal axes of x (n x d);
 // axes_out (optional) receives V_k (d x k, row-major). k <= 128, d <= 1024.

@@ -159,7 +159,36 @@ __global__ void normalize_center_kernel(const float* Y, uint64_t n, uint64_t d, 
   }
 }
 
+// One thread per row: the norm as ref_dist_sq(row, 0) (8 lane sums over chunks of 8 in order, the lanes
+// summed in order, then the tail), then every element divided by it.
+__global__ void normalize_rows_kernel(float* __restrict__ x, uint64_t n, int d) {
+  const uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  float* row = x + r * d;
+  float acc[8];
+#pragma unroll
+  for (int l = 0; l < 8; ++l) acc[l] = 0.0f;
+  const int nc = d >> 3;
+  for (int ch = 0; ch < nc; ++ch) {
+#pragma unroll
+    for (int l = 0; l < 8; ++l) acc[l] = __fadd_rn(acc[l], __fmul_rn(row[8 * ch + l], row[8 * ch + l]));
+  }
+  float t = 0.0f;
+#pragma unroll
+  for (int l = 0; l < 8; ++l) t = __fadd_rn(t, acc[l]);
+  for (int e = nc * 8; e < d; ++e) t = __fadd_rn(t, __fmul_rn(row[e], row[e]));
+  const float nrm = __fsqrt_rn(t);
+  if (!(nrm > 0.0f)) return;
+  for (int e = 0; e < d; ++e) row[e] = __fdiv_rn(row[e], nrm);
+}
+
 }  // namespace
+
+void normalize_rows_device(Ctx& c, float* d_x, uint64_t n, uint64_t d) {
+  if (!n || !d) return;
+  normalize_rows_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(d_x, n, static_cast<int>(d));
+  PM_LAUNCHED();
+}
 
 // y = (x - sub) / div with pitch dp = d rounded up to 4 floats (the TMA stride rule), written into
 // `dst` when that pitch is d and dst is 16-byte aligned (no scratch at all), else into Y; then the

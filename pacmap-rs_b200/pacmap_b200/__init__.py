@@ -25,7 +25,7 @@ from ._abi import ptr
 
 __all__ = [
     "Configuration", "Initialization", "PairConfiguration", "fit_transform", "fit_transform_device",
-    "PaCMapError", "KnnMode", "knn", "quality", "last_launch_count", "learned",
+    "PaCMapError", "KnnMode", "Metric", "knn", "quality", "last_launch_count", "learned",
 ]
 
 # ---------------------------------------------------------------------------------------------
@@ -132,6 +132,15 @@ class KnnMode:
     SIMT_EXACT = 3
 
 
+class Metric:
+    """The distance the pairs are drawn with (engine switch; the reference is Euclidean only,
+    README.md:164). ANGULAR: the preprocessed rows are scaled to unit norm, so distances become
+    sqrt(2 - 2 cos)."""
+
+    EUCLIDEAN = 0
+    ANGULAR = 1
+
+
 @dataclass
 class Configuration:
     """Configuration (lib.rs:159-224) with the reference's defaults, plus engine switches."""
@@ -150,6 +159,7 @@ class Configuration:
     # engine switches (no reference analogue)
     knn_mode: int = KnnMode.AUTO
     device: int = 0
+    metric: int = Metric.EUCLIDEAN
 
     @staticmethod
     def builder() -> "_Builder":
@@ -230,6 +240,7 @@ class _CConfig:
         c.approx_threshold = int(config.approx_threshold)
         c.knn_mode = int(config.knn_mode)
         c.device = int(config.device)
+        c.metric = int(config.metric)
         if loss_trace is not None:
             self.keep.append(loss_trace)
             c.loss_trace = loss_trace.ctypes.data

@@ -42,6 +42,7 @@ class Config(C.Structure):
         ("knn_mode", C.c_int32),
         ("device", C.c_int32),
         ("loss_trace", C.c_void_p),
+        ("metric", C.c_int32),
     ]
 
 

@@ -377,3 +377,49 @@ def test_pca_default_configuration_embeds_like_random_init(lib):
     xw = np.concatenate([x, 0.1 * np.random.default_rng(1).normal(size=(2000, 60)).astype(np.float32)], 1)
     y_w, _ = lib.fit_transform(xw, lib.Configuration(seed=42))
     assert np.all(np.isfinite(y_w)) and lib.quality(xw, y_w, sample, trip)[1] >= q_rnd[1] - 0.05
+
+
+# ----------------------------------------------------------------------------------------------------
+# The angular metric (engine switch; the reference is Euclidean only, README.md:164).
+# ----------------------------------------------------------------------------------------------------
+def _unit_rows(orc, xp):
+    out = xp.copy()
+    zero = np.zeros(xp.shape[1], np.float32)
+    for r in range(xp.shape[0]):
+        nrm = np.float32(orc.distance(xp[r], zero))  # the reference's f32 distance from the origin
+        if nrm > 0:
+            out[r] = (xp[r] / nrm).astype(np.float32)
+    return out
+
+
+def test_angular_pairs_are_the_euclidean_pairs_of_unit_rows(lib, orc):
+    x = _mixture(2000, 40, seed=12)
+    x *= np.random.default_rng(3).uniform(0.2, 5.0, size=(2000, 1)).astype(np.float32)  # scales vary
+    cfg = lib.Configuration(seed=7, initialization=lib.Initialization.Random(1), metric=lib.Metric.ANGULAR)
+    pnn, pmn, pfp = lib.stages.generate_pairs(x, cfg)
+    xp, *_ = orc.preprocess(x)
+    enn, emn, efp = orc.generate_pairs(_unit_rows(orc, xp), 10, 5, 20, 7)
+    assert np.array_equal(pnn, enn) and np.array_equal(pmn, emn) and np.array_equal(pfp, efp)
+    with pytest.raises(lib.InvalidArgument):
+        lib.stages.generate_pairs(x, lib.Configuration(seed=7, metric=5))
+
+
+def test_angular_neighbours_are_closer_in_angle(lib, orc):
+    """Rows with scales spread over two decades: the neighbour pairs drawn with the angular metric have
+    a higher cosine similarity (on the preprocessed rows) than the Euclidean ones, and most differ."""
+    rng = np.random.default_rng(8)
+    x = (_mixture(3000, 24, seed=9) * rng.uniform(0.1, 10.0, size=(3000, 1))).astype(np.float32)
+    R = lib.Initialization.Random(3)
+    p_ang = lib.stages.generate_pairs(x, lib.Configuration(seed=2, initialization=R, metric=lib.Metric.ANGULAR))[0]
+    p_euc = lib.stages.generate_pairs(x, lib.Configuration(seed=2, initialization=R))[0]
+    xp, *_ = orc.preprocess(x)
+    u = xp.astype(np.float64) / np.linalg.norm(xp.astype(np.float64), axis=1, keepdims=True)
+
+    def mean_cos(p):
+        return float((u[p[:, 0]] * u[p[:, 1]]).sum(1).mean())
+
+    c_ang, c_euc = mean_cos(p_ang), mean_cos(p_euc)
+    print(f"mean cosine of neighbour pairs: angular {c_ang:.4f}, euclidean {c_euc:.4f}")
+    assert c_ang > c_euc + 0.002  # measured 0.9732 vs 0.9697
+    same = (p_ang == p_euc).all(1).mean()
+    assert same < 0.5  # measured 0.136
