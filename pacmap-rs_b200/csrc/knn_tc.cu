@@ -193,50 +193,94 @@ __device__ __forceinline__ int warp_compact(uint32_t* __restrict__ idx, float* _
 //    order below) and its threshold tightens after a few tiles. Any order gives the same exact kNN.
 // ---------------------------------------------------------------------------------------------
 constexpr int PIV = 256;
-constexpr int PIV_CHUNK = 32;
 
+// Register-tiled: a block takes 64 points and the pivots in two passes of 128; each thread keeps 4
+// points x 8 pivots of dot products while d is staged through shared memory in slices of 32. Any
+// assignment order gives the same kNN; this one only has to be fast.
+constexpr int PA_PTS = 64, PA_PIV = 128, PA_D = 32;
 __global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restrict__ x, uint64_t n, int d,
                                                            uint32_t* __restrict__ cell, uint32_t* __restrict__ count) {
-  extern __shared__ float ps[];  // PIV_CHUNK x d pivots, then PIV_CHUNK norms
-  float* pn = ps + PIV_CHUNK * d;
-  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  __shared__ float xs[PA_D][PA_PTS + 4];  // [dim][point]
+  __shared__ float ps[PA_D][PA_PIV + 4];  // [dim][pivot]
+  __shared__ float pn[PA_PIV];
+  __shared__ float best_s[PA_PTS][16];
+  __shared__ uint32_t best_i[PA_PTS][16];
+  const uint64_t pt0 = static_cast<uint64_t>(blockIdx.x) * PA_PTS;
+  const int tp = threadIdx.x >> 4;  // 16 point groups of 4 points
+  const int tq = threadIdx.x & 15;  // 16 pivot groups of 8 pivots
   float best = __int_as_float(0x7f800000);
   uint32_t arg = 0;
-  for (int p0 = 0; p0 < PIV; p0 += PIV_CHUNK) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < PIV_CHUNK * d; e += blockDim.x) {
-      const int p = e / d, c = e - p * d;
-      ps[e] = x[(static_cast<uint64_t>(p0 + p) * n / PIV) * d + c];
-    }
-    __syncthreads();
-    if (threadIdx.x < PIV_CHUNK) {
-      float s = 0.0f;
-      for (int c = 0; c < d; ++c) s = fmaf(ps[threadIdx.x * d + c], ps[threadIdx.x * d + c], s);
-      pn[threadIdx.x] = s;
-    }
-    __syncthreads();
-    if (i < n) {
-      float dot[PIV_CHUNK];
+  for (int half = 0; half < PIV / PA_PIV; ++half) {
+    float acc[4][8];
 #pragma unroll
-      for (int p = 0; p < PIV_CHUNK; ++p) dot[p] = 0.0f;
-      for (int c = 0; c < d; ++c) {
-        const float xv = x[i * d + c];
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int p = 0; p < PIV_CHUNK; ++p) dot[p] = fmaf(xv, ps[p * d + c], dot[p]);
+      for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+    float nrm = 0.0f;  // thread t < 128: |pivot t|^2 of this half
+    for (int c0 = 0; c0 < d; c0 += PA_D) {
+      __syncthreads();
+      for (int e = threadIdx.x; e < PA_D * PA_PTS; e += 256) {
+        const int pi = e / PA_D, cc = e % PA_D;
+        const uint64_t r = pt0 + pi;
+        xs[cc][pi] = (r < n && c0 + cc < d) ? x[r * d + c0 + cc] : 0.0f;
       }
+      for (int e = threadIdx.x; e < PA_D * PA_PIV; e += 256) {
+        const int pv = e / PA_D, cc = e % PA_D;
+        const uint64_t prow = static_cast<uint64_t>(half * PA_PIV + pv) * n / PIV;
+        ps[cc][pv] = (c0 + cc < d) ? x[prow * d + c0 + cc] : 0.0f;
+      }
+      __syncthreads();
+      if (threadIdx.x < PA_PIV)
+        for (int cc = 0; cc < PA_D; ++cc) nrm = fmaf(ps[cc][threadIdx.x], ps[cc][threadIdx.x], nrm);
+#pragma unroll 8
+      for (int cc = 0; cc < PA_D; ++cc) {
+        float xv[4], pv[8];
 #pragma unroll
-      for (int p = 0; p < PIV_CHUNK; ++p) {
-        const float sc = fmaf(-2.0f, dot[p], pn[p]);
-        if (sc < best) {
+        for (int i = 0; i < 4; ++i) xv[i] = xs[cc][tp * 4 + i];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) pv[j] = ps[cc][tq * 8 + j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(xv[i], pv[j], acc[i][j]);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < PA_PIV) pn[threadIdx.x] = nrm;
+    __syncthreads();
+    // per point: the best of this thread's 8 pivots, then of the 16 threads sharing the point
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      float b = __int_as_float(0x7f800000);
+      uint32_t bi = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float sc = fmaf(-2.0f, acc[i][j], pn[tq * 8 + j]);
+        if (sc < b) {
+          b = sc;
+          bi = static_cast<uint32_t>(half * PA_PIV + tq * 8 + j);
+        }
+      }
+      best_s[tp * 4 + i][tq] = b;
+      best_i[tp * 4 + i][tq] = bi;
+    }
+    __syncthreads();
+    if (threadIdx.x < PA_PTS) {
+      for (int q = 0; q < 16; ++q) {
+        const float sc = best_s[threadIdx.x][q];
+        if (sc < best) {  // ascending pivot order: ties keep the lower pivot
           best = sc;
-          arg = static_cast<uint32_t>(p0 + p);
+          arg = best_i[threadIdx.x][q];
         }
       }
     }
   }
-  if (i < n) {
-    cell[i] = arg;
-    atomicAdd(&count[arg], 1u);
+  if (threadIdx.x < PA_PTS) {
+    const uint64_t i = pt0 + threadIdx.x;
+    if (i < n) {
+      cell[i] = arg;
+      atomicAdd(&count[arg], 1u);
+    }
   }
 }
 
@@ -283,10 +327,12 @@ __global__ void absmax_kernel(const float* __restrict__ x, uint64_t total, uint3
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// Also writes xperm (n x d, rows in the locality order), which the exact re-rank gathers from.
 template <bool BF16>
 __global__ void split_rows_kernel(const float* __restrict__ x, const uint32_t* __restrict__ perm, uint64_t n, int d,
                                   int KP, uint64_t n_pad, float s, uint16_t* __restrict__ H, float* __restrict__ nrm,
-                                  float* __restrict__ A, float* __restrict__ B, double* __restrict__ partial) {
+                                  float* __restrict__ A, float* __restrict__ B, double* __restrict__ partial,
+                                  float* __restrict__ xperm) {
   __shared__ double red[2][8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double sa = 0.0, sb = 0.0;
@@ -295,7 +341,11 @@ __global__ void split_rows_kernel(const float* __restrict__ x, const uint32_t* _
     const uint64_t src = r < n ? static_cast<uint64_t>(perm[r]) : 0;
     for (int c = lane; c < KP; c += 32) {
       float xs = 0.0f;
-      if (r < n && c < d) xs = x[src * d + c] * s;
+      if (r < n && c < d) {
+        const float xv = x[src * d + c];
+        xperm[r * d + c] = xv;
+        xs = xv * s;
+      }
       uint16_t hbits;
       float hf;
       if (BF16) {
@@ -690,6 +740,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
 //     groups in distance.rs:50-75's lane order, 4 survivors per warp pass, row i of x in registers
 //     when it has at most 8 * NC elements, else read from L1 each pass with NC = 0), sorted by
 //     (distance, index); output at the original row, original indices.
+// x: the rows in the locality order (row r is point perm[r]); candidates of nearby rows sit nearby.
 template <int PER, int WARPS, int NC>
 __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
     const float* __restrict__ x, uint64_t n, int d, int K, const uint32_t* __restrict__ perm,
@@ -707,7 +758,7 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
     if (m < 0) continue;  // overflowed in the filter: handled by the exact fallback
     const uint64_t rb = r * static_cast<uint64_t>(C);
     const uint64_t orow = perm[r];
-    const float* a = x + orow * d;
+    const float* a = x + r * d;
     float ra[NC > 0 ? NC : 1];
 #pragma unroll
     for (int ch = 0; ch < NC; ++ch) ra[ch] = ch < nc ? a[8 * ch + l8] : 0.0f;
@@ -716,7 +767,7 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
       const int e = e0 + grp;
       const uint32_t jp = (e < m) ? cand[rb + e].x : static_cast<uint32_t>(r);
       const uint32_t j = perm[jp];
-      const float* b = x + static_cast<uint64_t>(j) * d;
+      const float* b = x + static_cast<uint64_t>(jp) * d;
       float accl = 0.0f;
       if (NC > 0) {
 #pragma unroll
@@ -801,9 +852,8 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   // locality order
   DevBuf<uint32_t> cell(c, n), ccount(c, PIV), perm(c, n);
   PM_CUDA(cudaMemsetAsync(ccount.get(), 0, PIV * sizeof(uint32_t), c.stream));
-  const size_t psm = (static_cast<size_t>(PIV_CHUNK) * d + PIV_CHUNK) * sizeof(float);
-  PM_CUDA(cudaFuncSetAttribute(pivot_assign_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(psm)));
-  pivot_assign_kernel<<<ceil_div(n, 256), 256, psm, c.stream>>>(d_x, n, static_cast<int>(d), cell.get(), ccount.get());
+  pivot_assign_kernel<<<ceil_div(n, PA_PTS), 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), cell.get(),
+                                                                 ccount.get());
   PM_LAUNCHED();
   cell_offsets_kernel<<<1, 32, 0, c.stream>>>(ccount.get());
   PM_LAUNCHED();
@@ -811,6 +861,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_LAUNCHED();
 
   DevBuf<uint16_t> H(c, n_pad * KP);
+  DevBuf<float> xperm(c, n * d);
   DevBuf<float> nrm(c, n_pad), A(c, n_pad), B(c, n_pad);
   DevBuf<float2> ge(c, n_pad);
   DevBuf<uint16_t> gq(c, n_pad * 16);
@@ -818,10 +869,10 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   DevBuf<double> partial(c, 2 * sgrid);
   if (bf16)
     split_rows_kernel<true><<<sgrid, 256, 0, c.stream>>>(d_x, perm.get(), n, static_cast<int>(d), KP, n_pad, s, H.get(),
-                                                       nrm.get(), A.get(), B.get(), partial.get());
+                                                       nrm.get(), A.get(), B.get(), partial.get(), xperm.get());
   else
     split_rows_kernel<false><<<sgrid, 256, 0, c.stream>>>(d_x, perm.get(), n, static_cast<int>(d), KP, n_pad, s, H.get(),
-                                                        nrm.get(), A.get(), B.get(), partial.get());
+                                                        nrm.get(), A.get(), B.get(), partial.get(), xperm.get());
   PM_LAUNCHED();
   std::vector<double> hp(2 * sgrid);
   PM_CUDA(cudaMemcpyAsync(hp.data(), partial.get(), hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -916,8 +967,8 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   const int di = static_cast<int>(d), ki = static_cast<int>(kp);
   auto rerank = [&](auto kern, int warps) {
     const unsigned rgrid = std::min<unsigned>(ceil_div(n, warps), c.sm_count * 32);
-    kern<<<rgrid, warps * 32, 0, c.stream>>>(d_x, n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx, d_dist,
-                                             fbk.get(), fbk.get() + n);
+    kern<<<rgrid, warps * 32, 0, c.stream>>>(xperm.get(), n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
+                                             d_dist, fbk.get(), fbk.get() + n);
   };
   if (PER == 16) {
     if (d > 256) rerank(knn_rerank_kernel<16, 8, 0>, 8);
