@@ -263,9 +263,7 @@ struct Sched {
   float w_nn, w_mn, w_fp, lr_t;
 };
 
-// One row's entries: [s0, s1) NN, [s1, s2) MN (skipped when w_mn == 0), [s2, s3) FP, walked as one index
-// space q = gl, gl + G, ... (a fixed per-lane summation order) with a two-deep software pipeline:
-// while entry k is summed, y of entry k + 1 and the partner index of entry k + 2 are in flight.
+// y of partner j (DIM consecutive floats; one 8-byte load for 2-D).
 template <int DIM>
 __device__ __forceinline__ void load_y(const float* __restrict__ y, uint32_t j, float (&out)[DIM]) {
   if constexpr (DIM == 2) {
