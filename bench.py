@@ -360,7 +360,8 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"kernel": "knn_filter_kernel (tcgen05 distance GEMM + fused candidate filter)" if stages_learned.get("knn_filter") else "knn_simt_kernel", "bound": "tensor",
                      "achieved": round(achieved_tf, 2) if achieved_tf else None, "peak": bf16, "unit": "TFLOP/s",
                      "frac": round(achieved_tf / bf16, 4) if achieved_tf else None, "traffic": None,
-                     "peak_source": f"{src} bf16 dense", "algorithmic": "2*n^2*d flops per launch"},
+                     "peak_source": f"{src} bf16 dense", "algorithmic": "2*n^2*d flops per launch",
+                     "filter_rate_scores_per_s": round(n * n / (knn_ms * 1e-3), 1) if knn_ms > 0 else None},
         "roofline_optimizer": {"kernel": "grad_adam_kernel (CSR gradient + Adam, CUDA graph)", "bound": "hbm",
                                "achieved": round(opt_gbs, 1) if opt_gbs else None, "peak": hbm, "unit": "GB/s",
                                "frac": round(opt_gbs / hbm, 4) if opt_gbs else None,

@@ -220,6 +220,11 @@ pacmap_status pacmap_fit_transform_learned_device(const float* d_x, uint64_t n, 
                                                   const float* mlp_params, float* d_out_embedding,
                                                   float* d_out_snapshots);
 
+/* Initialization::Pca's eigen-step on the host (no GPU): the k leading eigenvectors of a symmetric
+ * d x d matrix (f64, row-major) into axes (d x k, row-major), by descending eigenvalue, each column's
+ * largest-magnitude entry positive. Cyclic Jacobi for d <= 160, else subspace iteration + Rayleigh-Ritz. */
+pacmap_status pacmap_pca_axes(const double* cov, uint64_t d, uint64_t k, double* out_axes);
+
 /* --- the learned model on disk and the transform of new points (no reference analogue: the reference
  * embeds only the points it was fitted on, README.md:165) ---
  * A model is the MLP above, its training data's preprocessing constants (pacmap_preprocess's min, max

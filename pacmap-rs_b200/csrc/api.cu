@@ -514,6 +514,13 @@ pacmap_status pacmap_mlp_apply(const float* params, uint64_t d, uint64_t dim, co
   });
 }
 
+pacmap_status pacmap_pca_axes(const double* cov, uint64_t d, uint64_t k, double* out_axes) {
+  return guarded([&] {
+    PM_REQUIRE(cov && out_axes, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    pca_top_axes(cov, d, k, out_axes);
+  });
+}
+
 pacmap_status pacmap_model_target_stats(const float* y, uint64_t n, uint64_t dim, float* out_mean, float* out_std) {
   return guarded([&] {
     PM_REQUIRE(y && out_mean && out_std, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");

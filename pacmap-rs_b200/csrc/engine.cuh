@@ -105,6 +105,9 @@ void normalize_rows_device(Ctx& c, float* d_x, uint64_t n, uint64_t d);
 // axes_out (optional) receives V_k (d x k, row-major). k <= 128, d <= 1024.
 void pca_project_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t k, float scale, float* d_out,
                         std::vector<float>* axes_out);
+// The k leading eigenvectors of a symmetric d x d matrix (host, f64): axes (d x k, row-major), by
+// descending eigenvalue, each column's largest-magnitude entry positive.
+void pca_top_axes(const double* cov, uint64_t d, uint64_t k, double* axes);
 // d_out (n x k) = scale * x[:, :k] for x (n x w).
 void leading_columns(Ctx& c, const float* d_x, uint64_t n, uint64_t w, uint64_t k, float scale, float* d_out);
 void init_random_device(Ctx& c, uint64_t n, uint64_t dim, uint64_t seed, float* d_y);

@@ -280,6 +280,13 @@ __global__ void leading_columns_kernel(const float* __restrict__ x, uint64_t n, 
 
 }  // namespace
 
+void pca_top_axes(const double* cov, uint64_t d, uint64_t k, double* axes) {
+  PM_REQUIRE(k >= 1 && k <= d && d <= 1024, PACMAP_ERR_UNSUPPORTED, "axes need 1 <= k <= d <= 1024");
+  std::vector<double> a(cov, cov + d * d);
+  const std::vector<double> V = top_axes(a, static_cast<int>(d), static_cast<int>(k));
+  std::copy(V.begin(), V.end(), axes);
+}
+
 void leading_columns(Ctx& c, const float* d_x, uint64_t n, uint64_t w, uint64_t k, float scale, float* d_out) {
   if (!n || !k) return;
   leading_columns_kernel<<<static_cast<unsigned>(std::min<uint64_t>(ceil_div(n * k, 256), c.sm_count * 16ull)), 256, 0,

@@ -20,6 +20,15 @@ def preprocess(x, device: int = 0):
     return out, mn.value, mx.value, mean
 
 
+def pca_axes(cov, k: int):
+    """Initialization::Pca's eigen-step (host): the k leading eigenvectors of a symmetric matrix (d x k)."""
+    cov = np.ascontiguousarray(cov, dtype=np.float64)
+    d = cov.shape[0]
+    out = np.zeros((d, k), np.float64)
+    _check(_abi.lib().pacmap_pca_axes(ptr(cov), d, k, ptr(out)))
+    return out
+
+
 def generate_pairs(x, config: Configuration):
     """sample_pairs with Generate (lib.rs:641-648 -> neighbors.rs:56-108) -> (pair_nn, pair_mn, pair_fp)."""
     x = np.ascontiguousarray(x, dtype=np.float32)

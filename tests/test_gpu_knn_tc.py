@@ -75,6 +75,16 @@ def _tc_vs_simt(lib, x, k):
     assert np.array_equal(gi, si)
 
 
+def test_tc_knn_anisotropic_100k_slice(lib):
+    # a 100,000-row slice of the 1M x 128 generator, preprocessed, k' = 90: the tensor-core filter against
+    # the exact SIMT path
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.anisotropic_mixture(n=100000, d=128, k=50, seed=0, draw_seed=5)
+    xp = lib.stages.preprocess(x)[0]
+    _tc_vs_simt(lib, xp, 90)
+
+
 def test_tc_knn_image_like_60k_x_784(lib):
     # the 60,000 x 784 image-like configuration (quantised to 1/255, many ties), k' = 22 + 50
     from pacmap_b200 import datasets
