@@ -139,6 +139,15 @@ pacmap_status pacmap_fit_transform_device(const float* d_x, uint64_t n, uint64_t
 pacmap_status pacmap_knn_exact(const float* x, uint64_t n, uint64_t d, uint64_t k, int32_t knn_mode,
                                int32_t device, uint32_t* out_idx, float* out_dist);
 
+/* One shard of pacmap_knn_exact for multi-GPU use (no reference analogue): every rank passes all
+ * points and computes the rows of shard `shard` of `n_shards` (the tensor-core path splits its row
+ * blocks in its locality order, the SIMT path the rows in order). out_idx, out_dist: n x k' with the
+ * shard's rows filled and the others zero; out_owned (n bytes): 1 on the rows filled. The shards of
+ * one (x, k, knn_mode) partition the rows, and their union is pacmap_knn_exact's output bit for bit. */
+pacmap_status pacmap_knn_exact_shard(const float* x, uint64_t n, uint64_t d, uint64_t k, int32_t knn_mode,
+                                     uint32_t shard, uint32_t n_shards, int32_t device, uint32_t* out_idx,
+                                     float* out_dist, uint8_t* out_owned);
+
 /* --- stage entry points: the parity harness and callers that run part of the pipeline --- */
 
 /* preprocess_x non-PCA branch (src/lib.rs:485-511): out = (x - min) / max - column mean. x, out: n x d.

@@ -599,6 +599,39 @@ pacmap_status pacmap_knn_exact(const float* x, uint64_t n, uint64_t d, uint64_t 
   });
 }
 
+pacmap_status pacmap_knn_exact_shard(const float* x, uint64_t n, uint64_t d, uint64_t k, int32_t knn_mode,
+                                     uint32_t shard, uint32_t n_shards, int32_t device, uint32_t* out_idx,
+                                     float* out_dist, uint8_t* out_owned) {
+  return guarded([&] {
+    PM_REQUIRE(n_shards >= 1 && shard < n_shards, PACMAP_ERR_INVALID_ARGUMENT, "shard must be < n_shards");
+    if (n == 0) return;
+    const uint64_t kp = std::min<uint64_t>(k, n - 1);
+    PM_REQUIRE(x && out_owned && (kp == 0 || (out_idx && out_dist)), PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
+    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 3, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
+    DeviceLock dl(device);
+    Ctx& c = dl.ctx;
+    DevBuf<float> dx, dd(c, n * kp);
+    DevBuf<uint32_t> di(c, n * kp);
+    DevBuf<uint8_t> own(c, n);
+    upload(c, dx, x, n * d);
+    PM_CUDA(cudaMemsetAsync(own.get(), 0, n, c.stream));
+    if (kp > 0) {
+      PM_CUDA(cudaMemsetAsync(di.get(), 0, di.bytes(), c.stream));
+      PM_CUDA(cudaMemsetAsync(dd.get(), 0, dd.bytes(), c.stream));
+      KnnShard sh;
+      sh.index = shard;
+      sh.count = n_shards;
+      sh.d_owned = own.get();
+      knn_exact_device(c, dx.get(), n, d, kp, knn_mode, di.get(), dd.get(), sh);
+      PM_CUDA(cudaMemcpyAsync(out_idx, di.get(), di.bytes(), cudaMemcpyDeviceToHost, c.stream));
+      PM_CUDA(cudaMemcpyAsync(out_dist, dd.get(), dd.bytes(), cudaMemcpyDeviceToHost, c.stream));
+    }
+    PM_CUDA(cudaMemcpyAsync(out_owned, own.get(), n, cudaMemcpyDeviceToHost, c.stream));
+    PM_CUDA(cudaStreamSynchronize(c.stream));
+    c.check_errors("knn shard");
+  });
+}
+
 pacmap_status pacmap_preprocess(const float* x, uint64_t n, uint64_t d, int32_t device, float* out, float* out_min,
                                 float* out_max, float* out_mean) {
   return guarded([&] {

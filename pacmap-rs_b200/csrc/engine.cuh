@@ -69,9 +69,16 @@ void preprocess_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float* 
 void column_mean_seq(Ctx& c, const float* d_x, uint64_t n, uint64_t d, float sub, float div, float* d_mean);
 
 // ---- knn.cu ----
+// One shard of the query rows (multi-GPU kNN: every rank holds all points and computes its shard).
+// The tensor-core path splits its row blocks (in the locality order), the SIMT path the rows in order;
+// d_owned (n bytes, may be NULL) is set to 1 on the rows this shard wrote.
+struct KnnShard {
+  uint32_t index = 0, count = 1;
+  uint8_t* d_owned = nullptr;
+};
 // Exact kNN (k' columns, ascending (f32 distance, index)) of the rows of d_x against all rows.
 void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, int mode, uint32_t* d_idx,
-                      float* d_dist);
+                      float* d_dist, const KnnShard& shard = KnnShard());
 // Exact kNN of a subset of rows (query ids in d_rows) against all rows.
 // scatter: results go to the rows' own places (row r -> d_idx[r * kp]) instead of list order.
 void knn_rows_simt(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, const uint32_t* d_rows,

@@ -219,18 +219,37 @@ void knn_rows_simt(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   }
 }
 
+__global__ void iota_rows_kernel(uint32_t* __restrict__ rows, uint64_t r0, uint64_t count,
+                                 uint8_t* __restrict__ owned) {
+  const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  rows[t] = static_cast<uint32_t>(r0 + t);
+  if (owned) owned[r0 + t] = 1;
+}
+
 void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, int mode, uint32_t* d_idx,
-                      float* d_dist) {
+                      float* d_dist, const KnnShard& shard) {
   if (n == 0 || kp == 0) return;
+  PM_REQUIRE(shard.count >= 1 && shard.index < shard.count, PACMAP_ERR_INVALID_ARGUMENT, "bad kNN shard");
   // AUTO uses the tensor cores once the O(n^2) part dominates; the TENSOR modes force them.
   const bool want_tc = (mode == PACMAP_KNN_TENSOR_F16 || mode == PACMAP_KNN_TENSOR_BF16) ||
                        (mode == PACMAP_KNN_AUTO && n >= 16384);
   if (want_tc && knn_tc_supported(n, d, kp)) {
-    if (knn_tc_device(c, d_x, n, d, kp, mode == PACMAP_KNN_TENSOR_BF16, d_idx, d_dist)) return;
+    if (knn_tc_device(c, d_x, n, d, kp, mode == PACMAP_KNN_TENSOR_BF16, d_idx, d_dist, shard)) return;
   }
   PM_REQUIRE(mode == PACMAP_KNN_AUTO || mode == PACMAP_KNN_SIMT_EXACT, PACMAP_ERR_UNSUPPORTED,
              "the tensor-core kNN does not support this shape (d <= 1024 and k' <= 447 are required)");
-  knn_rows_simt(c, d_x, n, d, kp, nullptr, n, d_idx, d_dist);
+  if (shard.count == 1) {
+    knn_rows_simt(c, d_x, n, d, kp, nullptr, n, d_idx, d_dist);
+    if (shard.d_owned) PM_CUDA(cudaMemsetAsync(shard.d_owned, 1, n, c.stream));
+    return;
+  }
+  const uint64_t r0 = n * shard.index / shard.count, r1 = n * (shard.index + 1) / shard.count;
+  if (r1 == r0) return;
+  DevBuf<uint32_t> rows(c, r1 - r0);
+  iota_rows_kernel<<<ceil_div(r1 - r0, 256), 256, 0, c.stream>>>(rows.get(), r0, r1 - r0, shard.d_owned);
+  PM_LAUNCHED();
+  knn_rows_simt(c, d_x, n, d, kp, rows.get(), r1 - r0, d_idx, d_dist, /*scatter=*/true);
 }
 
 }  // namespace pacmap

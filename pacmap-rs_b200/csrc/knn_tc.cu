@@ -451,7 +451,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const __grid_constant__ CUtensorMap hmap, const __grid_constant__ CUtensorMap gmap, uint64_t n, uint64_t n_pad,
     int kb_rt, uint32_t idesc, const float2* __restrict__ ge, const float* __restrict__ nrm,
     const uint32_t* __restrict__ perm, int rank, uint2* __restrict__ cand, int* __restrict__ cand_cnt,
-    uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err) {
+    uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err,
+    int block_offset) {
   using L = FilterLayout<KB, MODE>;
   constexpr int NST = L::NST;
   constexpr int C = 32 * PER;
@@ -470,7 +471,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
   TcShared* sh = reinterpret_cast<TcShared*>(st_smem + NST * L::STAGE);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint64_t row0 = static_cast<uint64_t>(blockIdx.x) * TC_BM;
+  const int blk = static_cast<int>(blockIdx.x) + block_offset;  // row block (a shard runs a range of them)
+  const uint64_t row0 = static_cast<uint64_t>(blk) * TC_BM;
   const int ntiles = static_cast<int>(n_pad / TC_BN);
 
   // A operand of the column-term MMA: bf16 1.0 in every element (every swizzle reads the same tile).
@@ -514,7 +516,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
       int issued = 0, s = 0, ph = 0;
       bool stop = false;
       for (int t = 0; t < ntiles && !stop; ++t) {
-        const int tile = sweep_tile(t, static_cast<int>(blockIdx.x), ntiles);
+        const int tile = sweep_tile(t, blk, ntiles);
         for (int ch = 0; ch < nch; ++ch) {
           if (issued >= NST && !mbar_wait(&sh->empty[s], ph ^ 1, abort_flag)) {
             stop = true;
@@ -660,7 +662,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         break;
       }
       tc_fence_after();
-      const int col0 = sweep_tile(t, static_cast<int>(blockIdx.x), ntiles) * TC_BN;
+      const int col0 = sweep_tile(t, blk, ntiles) * TC_BN;
       const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) + acc * 256 + half * 128;
 #pragma unroll
       for (int cp = 0; cp < 2; ++cp) {  // 64 columns per pass, two TMEM loads in flight
@@ -823,8 +825,14 @@ bool knn_tc_supported(uint64_t n, uint64_t d, uint64_t kp) {
   return d >= 1 && d <= 1024 && kp >= 1 && kp + 1 <= 448 && n >= 2 && n < (1ull << 31);
 }
 
+__global__ void mark_owned_kernel(const uint32_t* __restrict__ perm, uint64_t r0, uint64_t r1,
+                                  uint8_t* __restrict__ owned) {
+  const uint64_t r = r0 + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r < r1) owned[perm[r]] = 1;
+}
+
 bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, bool bf16, uint32_t* d_idx,
-                   float* d_dist) {
+                   float* d_dist, const KnnShard& shard) {
   if (!knn_tc_supported(n, d, kp)) return false;
   const int KB = static_cast<int>((d + 63) / 64);
   const int KP = 64 * KB;
@@ -917,15 +925,27 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_CUDA(cudaMemsetAsync(fbk.get() + n, 0, sizeof(uint32_t), c.stream));
 
   const uint32_t idesc = idesc_f16(bf16);
-  const unsigned grid = static_cast<unsigned>(n_pad / TC_BM);
+  // this shard's row blocks (in the locality order); the compaction and the re-rank skip the other rows
+  const uint64_t blocks = n_pad / TC_BM;
+  const uint64_t blk0 = blocks * shard.index / shard.count, blk1 = blocks * (shard.index + 1) / shard.count;
+  const unsigned grid = static_cast<unsigned>(blk1 - blk0);
+  if (shard.d_owned && blk1 > blk0) {
+    const uint64_t r0 = std::min<uint64_t>(blk0 * TC_BM, n), r1 = std::min<uint64_t>(blk1 * TC_BM, n);
+    if (r1 > r0) {
+      mark_owned_kernel<<<ceil_div(r1 - r0, 256), 256, 0, c.stream>>>(perm.get(), r0, r1, shard.d_owned);
+      PM_LAUNCHED();
+    }
+  }
   cudaEvent_t ev[2];
   PM_CUDA(cudaEventCreate(&ev[0]));
   PM_CUDA(cudaEventCreate(&ev[1]));
   PM_CUDA(cudaEventRecord(ev[0], c.stream));
   auto launch = [&](auto kern, size_t smem) {
     PM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    if (grid == 0) return;
     kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, KB, idesc, ge.get(), nrm.get(), perm.get(), rank,
-                                               cand.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err);
+                                               cand.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err,
+                                               static_cast<int>(blk0));
   };
   const bool p16 = PER == 16;
   if (mode == MODE_STREAM) {

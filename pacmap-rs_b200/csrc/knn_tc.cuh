@@ -7,7 +7,7 @@ namespace pacmap {
 bool knn_tc_supported(uint64_t n, uint64_t d, uint64_t kp);
 // Exact kNN through the tensor-core filter + FP32 re-rank; false when it declined the problem.
 bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, bool bf16, uint32_t* d_idx,
-                   float* d_dist);
+                   float* d_dist, const KnnShard& shard = KnnShard());
 // Rows of the last tensor-core kNN on this thread that needed the exact SIMT recomputation.
 uint64_t& last_tc_fallback_rows();
 // Device time (ms) of the last filter kernel launch on this thread (CUDA events on its stream).

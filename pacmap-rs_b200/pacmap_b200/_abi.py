@@ -54,6 +54,7 @@ _SIGS = {
     "pacmap_fit_transform": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp]),
     "pacmap_fit_transform_device": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp]),
     "pacmap_knn_exact": (C.c_int, [_vp, _u64, _u64, _u64, _i32, _i32, _vp, _vp]),
+    "pacmap_knn_exact_shard": (C.c_int, [_vp, _u64, _u64, _u64, _i32, C.c_uint32, C.c_uint32, _i32, _vp, _vp, _vp]),
     "pacmap_preprocess": (C.c_int, [_vp, _u64, _u64, _i32, _vp, _vp, _vp, _vp]),
     "pacmap_generate_pairs": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp, _vp, _vp]),
     "pacmap_reselect_neighbors": (C.c_int, [_vp, _vp, _u64, _u64, _u64, _i32, _vp, _vp]),

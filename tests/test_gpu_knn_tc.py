@@ -118,3 +118,20 @@ def test_tc_knn_fallback_rows_over_key_slices(lib, orc):
     gi, gd = lib.knn.find_k_nearest_neighbors(x, 60, knn_mode=F16)
     ei, ed = orc.knn_exact(x, 60)
     assert np.array_equal(gd, ed) and np.array_equal(gi, ei)
+
+
+@pytest.mark.parametrize("mode,n,d,k", [(F16, 3000, 40, 60), (AUTO, 20000, 24, 30), (3, 2500, 17, 12)])
+def test_knn_shards_partition_rows_and_reproduce_the_full_result(lib, mode, n, d, k):
+    # the multi-GPU primitive on one GPU: shards of the tensor-core path (row blocks in its locality
+    # order) and of the SIMT path (rows in order) partition the rows and rebuild the full kNN exactly
+    x = _mix(n, d, seed=n)
+    gi, gd = lib.knn.find_k_nearest_neighbors(x, k, knn_mode=mode)
+    cover = np.zeros(n, int)
+    ui, ud = np.zeros_like(gi), np.zeros_like(gd)
+    for s in range(3):
+        si, sd, own = lib.knn.find_k_nearest_neighbors_shard(x, k, s, 3, knn_mode=mode)
+        cover += own
+        ui[own], ud[own] = si[own], sd[own]
+        assert not si[~own].any() and not sd[~own].any()
+    assert (cover == 1).all()
+    assert np.array_equal(ui, gi) and np.array_equal(ud, gd)
