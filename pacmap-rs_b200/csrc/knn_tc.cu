@@ -199,7 +199,7 @@ constexpr int PIV = 256;
 // assignment order gives the same kNN; this one only has to be fast.
 constexpr int PA_PTS = 64, PA_PIV = 128, PA_D = 32;
 __global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restrict__ x, uint64_t n, int d,
-                                                           uint32_t* __restrict__ cell, uint32_t* __restrict__ count) {
+                                                           uint32_t* __restrict__ cell) {
   __shared__ float xs[PA_D][PA_PTS + 4];  // [dim][point]
   __shared__ float ps[PA_D][PA_PIV + 4];  // [dim][pivot]
   __shared__ float pn[PA_PIV];
@@ -277,27 +277,68 @@ __global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restri
   }
   if (threadIdx.x < PA_PTS) {
     const uint64_t i = pt0 + threadIdx.x;
-    if (i < n) {
-      cell[i] = arg;
-      atomicAdd(&count[arg], 1u);
+    if (i < n) cell[i] = arg;
+  }
+}
+
+// The points sorted by cell, stably (ascending index within a cell), so that the order -- and with it the
+// row blocks a kNN shard owns -- is the same on every call: per-chunk cell counts, their offsets in
+// (cell, chunk) order, then one warp per chunk placing its points in index order.
+constexpr uint32_t PL_CHUNK = 4096;
+__global__ void __launch_bounds__(256) cell_chunk_count_kernel(const uint32_t* __restrict__ cell, uint64_t n,
+                                                               uint32_t* __restrict__ counts) {
+  __shared__ uint32_t h[PIV];
+  for (int t = threadIdx.x; t < PIV; t += blockDim.x) h[t] = 0;
+  __syncthreads();
+  const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * PL_CHUNK, c1 = c0 + PL_CHUNK < n ? c0 + PL_CHUNK : n;
+  for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) atomicAdd(&h[cell[i]], 1u);  // a count: any order
+  __syncthreads();
+  for (int t = threadIdx.x; t < PIV; t += blockDim.x) counts[static_cast<uint64_t>(blockIdx.x) * PIV + t] = h[t];
+}
+
+__global__ void __launch_bounds__(PIV) cell_chunk_offsets_kernel(uint32_t* __restrict__ counts, uint32_t chunks) {
+  __shared__ uint32_t start[PIV];
+  const int t = threadIdx.x;  // one thread per cell
+  uint32_t total = 0;
+  for (uint32_t ch = 0; ch < chunks; ++ch) total += counts[static_cast<uint64_t>(ch) * PIV + t];
+  start[t] = total;
+  __syncthreads();
+  if (t == 0) {
+    uint32_t run = 0;
+    for (int p = 0; p < PIV; ++p) {
+      const uint32_t v = start[p];
+      start[p] = run;
+      run += v;
     }
   }
-}
-
-__global__ void cell_offsets_kernel(uint32_t* __restrict__ count) {  // exclusive scan of PIV counts, 1 thread
-  if (threadIdx.x != 0) return;
-  uint32_t run = 0;
-  for (int p = 0; p < PIV; ++p) {
-    const uint32_t c = count[p];
-    count[p] = run;
-    run += c;
+  __syncthreads();
+  uint32_t run = start[t];
+  for (uint32_t ch = 0; ch < chunks; ++ch) {
+    const uint32_t v = counts[static_cast<uint64_t>(ch) * PIV + t];
+    counts[static_cast<uint64_t>(ch) * PIV + t] = run;
+    run += v;
   }
 }
 
-__global__ void cell_place_kernel(const uint32_t* __restrict__ cell, uint64_t n, uint32_t* __restrict__ cursor,
-                                  uint32_t* __restrict__ perm) {
-  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < n) perm[atomicAdd(&cursor[cell[i]], 1u)] = static_cast<uint32_t>(i);
+__global__ void __launch_bounds__(32) cell_place_kernel(const uint32_t* __restrict__ cell, uint64_t n,
+                                                        const uint32_t* __restrict__ offsets,
+                                                        uint32_t* __restrict__ perm) {
+  __shared__ uint32_t off[PIV];
+  const int lane = threadIdx.x;
+  for (int t = lane; t < PIV; t += 32) off[t] = offsets[static_cast<uint64_t>(blockIdx.x) * PIV + t];
+  __syncwarp();
+  const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * PL_CHUNK, c1 = c0 + PL_CHUNK < n ? c0 + PL_CHUNK : n;
+  for (uint64_t base = c0; base < c1; base += 32) {
+    const uint64_t i = base + lane;
+    const bool valid = i < c1;
+    const uint32_t cl = valid ? cell[i] : 0xFFFFFFFFu;
+    const unsigned same = __match_any_sync(0xFFFFFFFFu, cl);
+    const int rank = __popc(same & ((1u << lane) - 1u));
+    if (valid) perm[off[cl] + rank] = static_cast<uint32_t>(i);
+    __syncwarp();
+    if (valid && lane == __ffs(same) - 1) off[cl] += __popc(same);
+    __syncwarp();
+  }
 }
 
 // Column tile visited at step t by row block b: first the window of W tiles around the block's own
@@ -858,14 +899,15 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   const float s = std::ldexp(1.0f, 13 - ex);
 
   // locality order
-  DevBuf<uint32_t> cell(c, n), ccount(c, PIV), perm(c, n);
-  PM_CUDA(cudaMemsetAsync(ccount.get(), 0, PIV * sizeof(uint32_t), c.stream));
-  pivot_assign_kernel<<<ceil_div(n, PA_PTS), 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), cell.get(),
-                                                                 ccount.get());
+  const uint32_t chunks = ceil_div(n, PL_CHUNK);
+  DevBuf<uint32_t> cell(c, n), cell_counts(c, static_cast<uint64_t>(chunks) * PIV), perm(c, n);
+  pivot_assign_kernel<<<ceil_div(n, PA_PTS), 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), cell.get());
   PM_LAUNCHED();
-  cell_offsets_kernel<<<1, 32, 0, c.stream>>>(ccount.get());
+  cell_chunk_count_kernel<<<chunks, 256, 0, c.stream>>>(cell.get(), n, cell_counts.get());
   PM_LAUNCHED();
-  cell_place_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(cell.get(), n, ccount.get(), perm.get());
+  cell_chunk_offsets_kernel<<<1, PIV, 0, c.stream>>>(cell_counts.get(), chunks);
+  PM_LAUNCHED();
+  cell_place_kernel<<<chunks, 32, 0, c.stream>>>(cell.get(), n, cell_counts.get(), perm.get());
   PM_LAUNCHED();
 
   DevBuf<uint16_t> H(c, n_pad * KP);
