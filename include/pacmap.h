@@ -73,7 +73,12 @@ typedef enum pacmap_knn_mode {
   PACMAP_KNN_AUTO = 0,         /* tensor-core filter when the dimension allows it, else SIMT exact   */
   PACMAP_KNN_TENSOR_F16 = 1,   /* tcgen05 FP16 distance GEMM filter + exact FP32 re-rank            */
   PACMAP_KNN_TENSOR_BF16 = 2,  /* tcgen05 BF16 distance GEMM filter + exact FP32 re-rank            */
-  PACMAP_KNN_SIMT_EXACT = 3    /* every distance in the reference's FP32 order on CUDA cores        */
+  PACMAP_KNN_SIMT_EXACT = 3,   /* every distance in the reference's FP32 order on CUDA cores        */
+  PACMAP_KNN_APPROX = 4        /* approximate at n >= approx_threshold (the reference's rule,
+                                * src/neighbors.rs:71): each row block searches only the 16 of 256
+                                * pivot cells nearest its own; returned distances stay exact. Below
+                                * the threshold (or below 16,384 rows, where the SIMT path runs) exact;
+                                * pacmap_knn_exact has no threshold: approximate whenever it can be. */
 } pacmap_knn_mode;
 
 /* The distance the pairs are drawn with (no reference analogue: the reference is Euclidean only,

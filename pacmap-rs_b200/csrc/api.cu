@@ -174,7 +174,7 @@ struct DevPairs {
 
 // neighbors.rs:56-108 generate_pairs on the preprocessed data (exact kNN at every n).
 void generate_pairs_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, const PairCounts& pc, uint64_t seed,
-                           int knn_mode, DevPairs& out, StageTimer* tm = nullptr) {
+                           int knn_mode, DevPairs& out, StageTimer* tm = nullptr, uint64_t approx_threshold = 0) {
   const uint64_t kp = std::min<uint64_t>(pc.k + 50, n - 1);
   const uint64_t k = std::min<uint64_t>(pc.k, n - 1);
   DevBuf<uint32_t> idx(c, n * kp);
@@ -182,7 +182,7 @@ void generate_pairs_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, co
   if (tm) tm->start(ST_KNN);
   last_tc_filter_ms() = 0.0;
   last_tc_fallback_rows() = 0;
-  knn_exact_device(c, d_xp, n, d, kp, knn_mode, idx.get(), dist.get());
+  knn_exact_device(c, d_xp, n, d, kp, knn_mode, idx.get(), dist.get(), KnnShard(), approx_threshold);
   if (tm) tm->stop(ST_KNN);
   if (tm && tm->on) {
     g_stage_ms.resize(ST_COUNT + 2, 0.0);
@@ -212,7 +212,7 @@ void validate_config(const pacmap_config* cfg) {
   PM_REQUIRE(cfg != nullptr, PACMAP_ERR_INVALID_ARGUMENT, "config is NULL");
   PM_REQUIRE(cfg->init_kind >= 0 && cfg->init_kind <= 2, PACMAP_ERR_INVALID_ARGUMENT, "unknown init_kind");
   PM_REQUIRE(cfg->pair_kind >= 0 && cfg->pair_kind <= 2, PACMAP_ERR_INVALID_ARGUMENT, "unknown pair_kind");
-  PM_REQUIRE(cfg->knn_mode >= 0 && cfg->knn_mode <= 3, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
+  PM_REQUIRE(cfg->knn_mode >= 0 && cfg->knn_mode <= 4, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
   PM_REQUIRE(cfg->metric == PACMAP_METRIC_EUCLIDEAN || cfg->metric == PACMAP_METRIC_ANGULAR,
              PACMAP_ERR_INVALID_ARGUMENT, "unknown metric");
 }
@@ -255,7 +255,7 @@ void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const 
   // lib.rs:629-692 sample_pairs
   DevPairs pairs;
   if (cfg.pair_kind == PACMAP_PAIRS_GENERATE) {
-    generate_pairs_device(c, xp.get(), n, dw, pc, seed, cfg.knn_mode, pairs, &tm);
+    generate_pairs_device(c, xp.get(), n, dw, pc, seed, cfg.knn_mode, pairs, &tm, cfg.approx_threshold);
   } else if (cfg.pair_kind == PACMAP_PAIRS_NEIGHBORS_PROVIDED) {
     const uint64_t expected = n * pc.k;
     if (cfg.pair_neighbors_rows != expected)
@@ -585,7 +585,7 @@ pacmap_status pacmap_knn_exact(const float* x, uint64_t n, uint64_t d, uint64_t 
     const uint64_t kp = std::min<uint64_t>(k, n - 1);
     if (kp == 0) return;
     PM_REQUIRE(x && out_idx && out_dist, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
-    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 3, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
+    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 4, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
     DeviceLock dl(device);
     Ctx& c = dl.ctx;
     DevBuf<float> dx, dd(c, n * kp);
@@ -607,7 +607,7 @@ pacmap_status pacmap_knn_exact_shard(const float* x, uint64_t n, uint64_t d, uin
     if (n == 0) return;
     const uint64_t kp = std::min<uint64_t>(k, n - 1);
     PM_REQUIRE(x && out_owned && (kp == 0 || (out_idx && out_dist)), PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
-    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 3, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
+    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 4, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
     DeviceLock dl(device);
     Ctx& c = dl.ctx;
     DevBuf<float> dx, dd(c, n * kp);
@@ -666,7 +666,8 @@ pacmap_status pacmap_generate_pairs(const float* x, uint64_t n, uint64_t d, cons
     upload(c, dx, x, n * d);
     const uint64_t dw = preprocess_for(c, dx.get(), n, d, *cfg, false, xp);
     DevPairs pairs;
-    generate_pairs_device(c, xp.get(), n, dw, pc, cfg->has_seed ? cfg->seed : entropy_seed(), cfg->knn_mode, pairs);
+    generate_pairs_device(c, xp.get(), n, dw, pc, cfg->has_seed ? cfg->seed : entropy_seed(), cfg->knn_mode, pairs,
+                          nullptr, cfg->approx_threshold);
     if (out_pnn) PM_CUDA(cudaMemcpyAsync(out_pnn, pairs.nn.get(), pairs.nn.bytes(), cudaMemcpyDeviceToHost, c.stream));
     if (out_pmn) PM_CUDA(cudaMemcpyAsync(out_pmn, pairs.mn.get(), pairs.mn.bytes(), cudaMemcpyDeviceToHost, c.stream));
     if (out_pfp) PM_CUDA(cudaMemcpyAsync(out_pfp, pairs.fp.get(), pairs.fp.bytes(), cudaMemcpyDeviceToHost, c.stream));

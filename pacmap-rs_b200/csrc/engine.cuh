@@ -77,8 +77,9 @@ struct KnnShard {
   uint8_t* d_owned = nullptr;
 };
 // Exact kNN (k' columns, ascending (f32 distance, index)) of the rows of d_x against all rows.
+// mode PACMAP_KNN_APPROX searches approximately when n >= approx_threshold (exactly below it).
 void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, int mode, uint32_t* d_idx,
-                      float* d_dist, const KnnShard& shard = KnnShard());
+                      float* d_dist, const KnnShard& shard = KnnShard(), uint64_t approx_threshold = 0);
 // Exact kNN of a subset of rows (query ids in d_rows) against all rows.
 // scatter: results go to the rows' own places (row r -> d_idx[r * kp]) instead of list order.
 void knn_rows_simt(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, const uint32_t* d_rows,

@@ -228,16 +228,19 @@ __global__ void iota_rows_kernel(uint32_t* __restrict__ rows, uint64_t r0, uint6
 }
 
 void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, int mode, uint32_t* d_idx,
-                      float* d_dist, const KnnShard& shard) {
+                      float* d_dist, const KnnShard& shard, uint64_t approx_threshold) {
   if (n == 0 || kp == 0) return;
   PM_REQUIRE(shard.count >= 1 && shard.index < shard.count, PACMAP_ERR_INVALID_ARGUMENT, "bad kNN shard");
   // AUTO uses the tensor cores once the O(n^2) part dominates; the TENSOR modes force them.
+  const bool approx = mode == PACMAP_KNN_APPROX && n >= approx_threshold;
   const bool want_tc = (mode == PACMAP_KNN_TENSOR_F16 || mode == PACMAP_KNN_TENSOR_BF16) ||
-                       (mode == PACMAP_KNN_AUTO && n >= 16384);
+                       ((mode == PACMAP_KNN_AUTO || mode == PACMAP_KNN_APPROX) && n >= 16384);
   if (want_tc && knn_tc_supported(n, d, kp)) {
-    if (knn_tc_device(c, d_x, n, d, kp, mode == PACMAP_KNN_TENSOR_BF16, d_idx, d_dist, shard)) return;
+    if (knn_tc_device(c, d_x, n, d, kp, mode == PACMAP_KNN_TENSOR_BF16, d_idx, d_dist, shard, approx ? 16 : 0))
+      return;
   }
-  PM_REQUIRE(mode == PACMAP_KNN_AUTO || mode == PACMAP_KNN_SIMT_EXACT, PACMAP_ERR_UNSUPPORTED,
+  PM_REQUIRE(mode == PACMAP_KNN_AUTO || mode == PACMAP_KNN_SIMT_EXACT || mode == PACMAP_KNN_APPROX,
+             PACMAP_ERR_UNSUPPORTED,
              "the tensor-core kNN does not support this shape (d <= 1024 and k' <= 447 are required)");
   if (shard.count == 1) {
     knn_rows_simt(c, d_x, n, d, kp, nullptr, n, d_idx, d_dist);

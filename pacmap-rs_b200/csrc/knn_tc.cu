@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -493,7 +494,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     int kb_rt, uint32_t idesc, const float2* __restrict__ ge, const float* __restrict__ nrm,
     const uint32_t* __restrict__ perm, int rank, uint2* __restrict__ cand, int* __restrict__ cand_cnt,
     uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err,
-    int block_offset) {
+    int block_offset, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_list) {
   using L = FilterLayout<KB, MODE>;
   constexpr int NST = L::NST;
   constexpr int C = 32 * PER;
@@ -515,6 +516,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
   const int blk = static_cast<int>(blockIdx.x) + block_offset;  // row block (a shard runs a range of them)
   const uint64_t row0 = static_cast<uint64_t>(blk) * TC_BM;
   const int ntiles = static_cast<int>(n_pad / TC_BN);
+  // the column tiles this block visits: all of them in the sweep order, or (approximate kNN) its list
+  const uint32_t lbase = tile_ptr ? tile_ptr[blk] : 0u;
+  const int nt = tile_ptr ? static_cast<int>(tile_ptr[blk + 1] - lbase) : ntiles;
+  auto tile_at = [&](int t) -> int {
+    return tile_ptr ? static_cast<int>(tile_list[lbase + t]) : sweep_tile(t, blk, ntiles);
+  };
 
   // A operand of the column-term MMA: bf16 1.0 in every element (every swizzle reads the same tile).
   for (int e = threadIdx.x; e < G_BYTES / 4; e += TC_THREADS) reinterpret_cast<uint32_t*>(one_smem)[e] = 0x3F803F80u;
@@ -553,11 +560,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
           for (int kb = 0; kb < KB; ++kb)
             tma_load_2d(a_smem + (h * KB + kb) * KB_BYTES, &hmap, &sh->a_full, kb * 64, static_cast<int>(row0 + h * 128));
       }
-      const int total = ntiles * nch;
+      const int total = nt * nch;
       int issued = 0, s = 0, ph = 0;
       bool stop = false;
-      for (int t = 0; t < ntiles && !stop; ++t) {
-        const int tile = sweep_tile(t, blk, ntiles);
+      for (int t = 0; t < nt && !stop; ++t) {
+        const int tile = tile_at(t);
         for (int ch = 0; ch < nch; ++ch) {
           if (issued >= NST && !mbar_wait(&sh->empty[s], ph ^ 1, abort_flag)) {
             stop = true;
@@ -603,7 +610,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
       const uint64_t ones = sdesc_sw32(smem_u32(one_smem));
       const uint32_t idesc_col = idesc_f16(true);  // the column term is bf16 x bf16
       int s = 0, ph = 0;
-      for (int t = 0; ok && t < ntiles; ++t) {
+      for (int t = 0; ok && t < nt; ++t) {
         const int acc = t & 1;
         for (int ch = 0; ch < nch; ++ch) {
           if (!mbar_wait(&sh->full[s], ph, abort_flag)) {
@@ -696,14 +703,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         }
       }
     };
-    for (int t = 0; t < ntiles; ++t) {
+    for (int t = 0; t < nt; ++t) {
       const int acc = t & 1;
       if (!mbar_wait(&sh->tmem_full[acc], (t >> 1) & 1, abort_flag)) {
         ok = false;
         break;
       }
       tc_fence_after();
-      const int col0 = sweep_tile(t, blk, ntiles) * TC_BN;
+      const int col0 = tile_at(t) * TC_BN;
       const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) + acc * 256 + half * 128;
 #pragma unroll
       for (int cp = 0; cp < 2; ++cp) {  // 64 columns per pass, two TMEM loads in flight
@@ -866,6 +873,13 @@ bool knn_tc_supported(uint64_t n, uint64_t d, uint64_t kp) {
   return d >= 1 && d <= 1024 && kp >= 1 && kp + 1 <= 448 && n >= 2 && n < (1ull << 31);
 }
 
+// The pivots' rows (pivot p is point p * n / PIV) into a PIV x d array.
+__global__ void gather_pivots_kernel(const float* __restrict__ x, uint64_t n, int d, float* __restrict__ out) {
+  const int p = blockIdx.x;
+  const uint64_t row = static_cast<uint64_t>(p) * n / PIV;
+  for (int c = threadIdx.x; c < d; c += blockDim.x) out[static_cast<uint64_t>(p) * d + c] = x[row * d + c];
+}
+
 __global__ void mark_owned_kernel(const uint32_t* __restrict__ perm, uint64_t r0, uint64_t r1,
                                   uint8_t* __restrict__ owned) {
   const uint64_t r = r0 + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -873,7 +887,7 @@ __global__ void mark_owned_kernel(const uint32_t* __restrict__ perm, uint64_t r0
 }
 
 bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, bool bf16, uint32_t* d_idx,
-                   float* d_dist, const KnnShard& shard) {
+                   float* d_dist, const KnnShard& shard, int nprobe) {
   if (!knn_tc_supported(n, d, kp)) return false;
   const int KB = static_cast<int>((d + 63) / 64);
   const int KP = 64 * KB;
@@ -909,6 +923,62 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_LAUNCHED();
   cell_place_kernel<<<chunks, 32, 0, c.stream>>>(cell.get(), n, cell_counts.get(), perm.get());
   PM_LAUNCHED();
+
+  // Approximate kNN: every row block visits only the column tiles of the nprobe cells whose pivots are
+  // nearest its own cells' (own cells first), instead of every tile. The cells are contiguous ranges of
+  // the locality order: cell p starts at the first chunk's offset for p.
+  DevBuf<uint32_t> tile_ptr, tile_list;
+  if (nprobe > 0 && nprobe < PIV) {
+    std::vector<uint32_t> cstart(PIV + 1);
+    DevBuf<float> piv(c, static_cast<uint64_t>(PIV) * d);
+    gather_pivots_kernel<<<PIV, 128, 0, c.stream>>>(d_x, n, static_cast<int>(d), piv.get());
+    PM_LAUNCHED();
+    std::vector<float> hp(static_cast<size_t>(PIV) * d);
+    PM_CUDA(cudaMemcpyAsync(cstart.data(), cell_counts.get(), PIV * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+    PM_CUDA(cudaMemcpyAsync(hp.data(), piv.get(), hp.size() * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    PM_CUDA(cudaStreamSynchronize(c.stream));
+    cstart[PIV] = static_cast<uint32_t>(n);
+    // nearest pivots of each pivot (itself first), by f64 squared distance, ties to the lower index
+    std::vector<std::vector<int>> probe(PIV);
+    std::vector<std::pair<double, int>> dd(PIV);
+    for (int p = 0; p < PIV; ++p) {
+      for (int q = 0; q < PIV; ++q) {
+        double acc = 0.0;
+        for (uint64_t k = 0; k < d; ++k) {
+          const double df = static_cast<double>(hp[p * d + k]) - hp[q * d + k];
+          acc += df * df;
+        }
+        dd[q] = {q == p ? -1.0 : acc, q};
+      }
+      std::partial_sort(dd.begin(), dd.begin() + nprobe, dd.end());
+      for (int r = 0; r < nprobe; ++r) probe[p].push_back(dd[r].second);
+    }
+    const uint64_t nblocks = n_pad / TC_BM, ntl = n_pad / TC_BN;
+    std::vector<uint32_t> ptr(nblocks + 1, 0), list;
+    std::vector<uint64_t> stamp(ntl, ~0ull);
+    list.reserve(nblocks * static_cast<uint64_t>(nprobe) * 40);
+    auto add_cell = [&](int q, uint64_t b) {
+      if (cstart[q + 1] <= cstart[q]) return;
+      for (uint64_t t = cstart[q] / TC_BN; t <= (cstart[q + 1] - 1) / TC_BN; ++t)
+        if (stamp[t] != b) {
+          stamp[t] = b;
+          list.push_back(static_cast<uint32_t>(t));
+        }
+    };
+    for (uint64_t b = 0; b < nblocks; ++b) {
+      const uint64_t r0 = b * TC_BM, r1 = std::min<uint64_t>(r0 + TC_BM, n);
+      std::vector<int> own;
+      for (int p = 0; p < PIV && r0 < r1; ++p)
+        if (cstart[p] < r1 && cstart[p + 1] > r0) own.push_back(p);
+      for (int p : own) add_cell(p, b);
+      for (int r = 1; r < nprobe; ++r)
+        for (int p : own) add_cell(probe[p][r], b);
+      ptr[b + 1] = static_cast<uint32_t>(list.size());
+    }
+    if (list.empty()) list.push_back(0);
+    upload(c, tile_ptr, ptr.data(), ptr.size());
+    upload(c, tile_list, list.data(), list.size());
+  }
 
   DevBuf<uint16_t> H(c, n_pad * KP);
   DevBuf<float> xperm(c, n * d);
@@ -987,7 +1057,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     if (grid == 0) return;
     kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, KB, idesc, ge.get(), nrm.get(), perm.get(), rank,
                                                cand.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err,
-                                               static_cast<int>(blk0));
+                                               static_cast<int>(blk0), tile_ptr.get(), tile_list.get());
   };
   const bool p16 = PER == 16;
   if (mode == MODE_STREAM) {

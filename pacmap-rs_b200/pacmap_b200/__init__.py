@@ -130,6 +130,7 @@ class KnnMode:
     TENSOR_F16 = 1
     TENSOR_BF16 = 2
     SIMT_EXACT = 3
+    APPROX = 4  # approximate at n >= approx_threshold (16 of 256 pivot cells per row block); exact below
 
 
 class Metric:

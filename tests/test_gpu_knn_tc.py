@@ -135,3 +135,38 @@ def test_knn_shards_partition_rows_and_reproduce_the_full_result(lib, mode, n, d
         assert not si[~own].any() and not sd[~own].any()
     assert (cover == 1).all()
     assert np.array_equal(ui, gi) and np.array_equal(ud, gd)
+
+
+APPROX = 4
+
+
+def test_approximate_knn_recall_and_exact_distances(lib, orc):
+    """knn_mode APPROX: each row block searches the 16 pivot cells nearest its own. Most true neighbours
+    are found, every returned distance is the reference's exact f32 distance of that pair, and rank by
+    rank the returned distances are never below the exact ones."""
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.anisotropic_mixture(n=60000, d=32, k=20, seed=3)
+    xp = lib.stages.preprocess(x)[0]
+    k = 30
+    ei, ed = lib.knn.find_k_nearest_neighbors(xp, k)
+    ai, ad = lib.knn.find_k_nearest_neighbors(xp, k, knn_mode=APPROX)
+    recall = np.mean([len(np.intersect1d(ai[r], ei[r])) / k for r in range(0, 60000, 7)])
+    print(f"approximate kNN recall {recall:.4f}")
+    assert recall >= 0.95
+    assert (ad >= ed).all() and (np.diff(ad, axis=1) >= 0).all()
+    rows = np.arange(0, 60000, 997)
+    for r in rows:
+        for c in range(0, k, 7):
+            assert ad[r, c] == np.float32(orc.distance(xp[r], xp[ai[r, c]]))
+
+
+def test_approximate_mode_is_exact_below_the_threshold(lib):
+    x = _mix(3000, 20, seed=5)
+    cfg = lambda thr: lib.Configuration(seed=7, initialization=lib.Initialization.Random(1), knn_mode=APPROX,  # noqa
+                                        approx_threshold=thr)
+    exact = lib.stages.generate_pairs(x, lib.Configuration(seed=7, initialization=lib.Initialization.Random(1)))
+    below = lib.stages.generate_pairs(x, cfg(8000))
+    assert all(np.array_equal(a, b) for a, b in zip(exact, below))
+    y, _ = lib.fit_transform(x, cfg(1000))  # above the threshold (SIMT at this n: still exact)
+    assert np.all(np.isfinite(y))
