@@ -165,6 +165,85 @@ __global__ void sample_fp_reg_kernel(const uint32_t* __restrict__ pnn, uint64_t 
   }
 }
 
+// sample_fp_pair_deterministic 32 stream words at a time (k <= 64, n_fp <= 96, n < 2^31): lane L takes
+// word pos + L of the point's stream (its own Philox block), applies the zone rule, and tests the value
+// against i, the k neighbours and the earlier picks (both in shared memory); among the lanes that pass,
+// only the first lane of each value counts (__match_any_sync), and the accepted lanes fill the slots
+// in lane order. The words counted as used end at the lane that filled the last slot. This is the
+// sequential rule of sample_fp_reg_kernel -- same picks, same order, same attempt budget -- with the
+// per-draw votes replaced by independent work across the lanes.
+constexpr int FPB_WARPS = 8, FPB_K = 64, FPB_P = 96;
+__global__ void __launch_bounds__(FPB_WARPS * 32) sample_fp_batch_kernel(const uint32_t* __restrict__ pnn, uint64_t n,
+                                                                         uint32_t k, uint32_t n_fp, uint64_t seed,
+                                                                         uint32_t* __restrict__ out,
+                                                                         uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_rej[FPB_WARPS][FPB_K];
+  __shared__ uint32_t s_pk[FPB_WARPS][FPB_P];
+  const int warp = threadIdx.x >> 5;
+  const uint32_t lane = lane_id();
+  uint32_t* rej = s_rej[warp];
+  uint32_t* pk = s_pk[warp];
+  const uint32_t range = static_cast<uint32_t>(n);
+  const uint32_t zone = (range << __clz(range)) - 1u;
+  const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * FPB_WARPS;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * FPB_WARPS + warp; i < n; i += warps) {
+    __syncwarp();
+    for (uint32_t t = lane; t < k; t += 32) rej[t] = pnn[((i * k) + t) * 2 + 1];
+    __syncwarp();
+    bool hit = false;
+    for (uint32_t t = lane; t < k; t += 32) hit |= rej[t] == static_cast<uint32_t>(i);
+    const bool self_in = __any_sync(0xFFFFFFFFu, hit);
+    uint64_t avail = n > k ? n - k : 0;
+    const uint64_t self_cut = self_in ? 0 : 1;
+    avail = avail > self_cut ? avail - self_cut : 0;
+    const uint32_t want = static_cast<uint32_t>((n_fp < avail ? static_cast<uint64_t>(n_fp) : avail));
+    const uint32_t c1 = static_cast<uint32_t>(i), c2 = static_cast<uint32_t>(i >> 32);
+    uint64_t pos = 0, budget = SAMPLE_ATTEMPT_CAP;
+    uint32_t cnt = 0;
+    while (cnt < want) {
+      if (budget == 0) {
+        if (lane == 0) atomicOr(err, DEV_ERR_SAMPLING);
+        break;
+      }
+      const uint32_t avail_w = budget < 32 ? static_cast<uint32_t>(budget) : 32u;
+      const uint64_t g = pos + lane;
+      uint32_t w4[4];
+      philox4x32_10(static_cast<uint32_t>(g >> 2), c1, c2, TAG_SAMPLE, k0, k1, w4);
+      const uint32_t e = static_cast<uint32_t>(g & 3);
+      const uint32_t w = e == 0 ? w4[0] : (e == 1 ? w4[1] : (e == 2 ? w4[2] : w4[3]));
+      const uint32_t j = __umulhi(w, range);
+      bool cand = lane < avail_w && w * range <= zone && j != static_cast<uint32_t>(i);
+      if (__any_sync(0xFFFFFFFFu, cand)) {
+        for (uint32_t t = 0; t < k; ++t) cand = cand && rej[t] != j;
+        for (uint32_t t = 0; t < cnt; ++t) cand = cand && pk[t] != j;
+      }
+      const uint32_t key = cand ? j : (0x80000000u | lane);  // j < 2^31: sentinels never match a value
+      const unsigned same = __match_any_sync(0xFFFFFFFFu, key);
+      const bool acc = cand && lane == static_cast<uint32_t>(__ffs(same) - 1);
+      const unsigned accm = __ballot_sync(0xFFFFFFFFu, acc);
+      const uint32_t need = want - cnt, got = __popc(accm);
+      const uint32_t rank = __popc(accm & ((1u << lane) - 1u));
+      if (acc && rank < need) {
+        pk[cnt + rank] = j;
+        out[(i * n_fp + cnt + rank) * 2 + 0] = static_cast<uint32_t>(i);
+        out[(i * n_fp + cnt + rank) * 2 + 1] = j;
+      }
+      uint32_t used = avail_w;
+      if (got >= need) {
+        const unsigned last = __ballot_sync(0xFFFFFFFFu, acc && rank == need - 1);
+        used = static_cast<uint32_t>(__ffs(last));  // through the lane that filled the last slot
+        cnt = want;
+      } else {
+        cnt += got;
+      }
+      pos += used;
+      budget -= used;
+      __syncwarp();
+    }
+  }
+}
+
 // The reference's f32 distance between rows a and b computed by an 8-lane group (l8 = lane % 8):
 // lane l8 forms the lane accumulator l8 of distance.rs:60-66, the group sums them in order 0..7,
 // adds the serial tail and takes the square root. Every lane of the group returns the result.
@@ -425,7 +504,9 @@ void sample_fp_device(Ctx& c, const uint32_t* d_pnn, uint64_t n, uint64_t k, uin
   PM_CUDA(cudaMemsetAsync(d_pfp, 0, n * n_fp * 2 * sizeof(uint32_t), c.stream));
   const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n, 8), c.sm_count * 32ull));
   const uint32_t k32 = static_cast<uint32_t>(k), f32n = static_cast<uint32_t>(n_fp);
-  if (n_fp <= 96 && k <= 64)
+  if (n_fp <= static_cast<uint64_t>(FPB_P) && k <= static_cast<uint64_t>(FPB_K) && n < (1ull << 31))
+    sample_fp_batch_kernel<<<grid, FPB_WARPS * 32, 0, c.stream>>>(d_pnn, n, k32, f32n, seed, d_pfp, c.d_err);
+  else if (n_fp <= 96 && k <= 64)
     sample_fp_reg_kernel<3, 2><<<grid, 256, 0, c.stream>>>(d_pnn, n, k32, f32n, seed, d_pfp, c.d_err);
   else if (n_fp <= 256 && k <= 128)
     sample_fp_reg_kernel<8, 4><<<grid, 256, 0, c.stream>>>(d_pnn, n, k32, f32n, seed, d_pfp, c.d_err);
