@@ -67,6 +67,7 @@ def lib():
         "orc_preprocess": (C.c_int, [_f32p, _u64, _u64, _f32p, _vp, _vp, _vp]),
         "orc_knn_exact": (C.c_int, [_f32p, _u64, _u64, _u64, _u32p, _f32p]),
         "orc_knn_exact_allpairs": (C.c_int, [_f32p, _u64, _u64, _u64, _u32p, _f32p]),
+        "orc_knn_rows": (C.c_int, [_f32p, _u64, _u64, _u32p, _u64, _u64, _u32p, _f32p]),
         "orc_sigma": (None, [_f32p, _u64, _u64, _f32p]),
         "orc_scale_dist": (None, [_f32p, _f32p, _u32p, _u64, _u64, _f32p]),
         "orc_sample_neighbors_pair": (None, [_f32p, _u32p, _u64, _u64, _u64, _u32p]),
@@ -164,6 +165,18 @@ def knn_exact(x, k: int, allpairs: bool = False):
     dist = np.zeros((n, kp), np.float32)
     fn = lib().orc_knn_exact_allpairs if allpairs else lib().orc_knn_exact
     _check(fn(x, n, d, k, idx, dist), "knn_exact")
+    return idx, dist
+
+
+def knn_rows(x, rows, k: int):
+    """Rows ``rows`` of ``knn_exact(x, k)`` (same indices and f32 distances), without the full matrix."""
+    x = _f32(x)
+    n, d = x.shape
+    rows = _u32(rows)
+    kp = min(k, n - 1) if n > 0 else 0
+    idx = np.zeros((rows.size, kp), np.uint32)
+    dist = np.zeros((rows.size, kp), np.float32)
+    _check(lib().orc_knn_rows(x, n, d, rows, rows.size, k, idx, dist), "knn_rows")
     return idx, dist
 
 

@@ -303,6 +303,61 @@ int orc_knn_exact(const float* x, uint64_t n, uint64_t d, uint64_t k, uint32_t* 
   return ORC_OK;
 }
 
+// knn.rs:137-194 for a subset of query rows: out row q holds the k'=min(k,n-1) smallest f32
+// distances from rows[q] to every j != rows[q], ordered by (distance, j) -- exactly row rows[q] of
+// orc_knn_exact, without the O(n^2 d) full matrix. Rows go in groups of 8 against chunks of 2,048
+// points, so each chunk is read from memory once per group; every row keeps its k' best (distance
+// key, index) pairs in a max-heap.
+int orc_knn_rows(const float* x, uint64_t n, uint64_t d, const uint32_t* rows, uint64_t m, uint64_t k, uint32_t* idx,
+                 float* dist) {
+  if (n == 0 || m == 0) return ORC_OK;
+  for (uint64_t q = 0; q < m; ++q)
+    if (rows[q] >= n) return ORC_ERR_INVALID_ARGUMENT;
+  const uint64_t kp = std::min<uint64_t>(k, n - 1);
+  if (kp == 0) return ORC_OK;
+  constexpr uint64_t G = 8, CH = 2048;
+  const int64_t groups = static_cast<int64_t>((m + G - 1) / G);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t g = 0; g < groups; ++g) {
+    const uint64_t q0 = static_cast<uint64_t>(g) * G, q1 = std::min<uint64_t>(q0 + G, m);
+    std::vector<std::vector<uint64_t>> heap(q1 - q0);
+    for (auto& h : heap) h.reserve(kp + 1);
+    for (uint64_t j0 = 0; j0 < n; j0 += CH) {
+      const uint64_t j1 = std::min<uint64_t>(j0 + CH, n);
+      for (uint64_t q = q0; q < q1; ++q) {
+        const uint64_t i = rows[q];
+        std::vector<uint64_t>& h = heap[q - q0];
+        for (uint64_t j = j0; j < j1; ++j) {
+          if (j == i) continue;
+          const float dd = ref_dist(x + i * d, x + j * d, d);
+          const uint64_t key = (static_cast<uint64_t>(total_key(dd)) << 32) | j;
+          if (h.size() < kp) {
+            h.push_back(key);
+            std::push_heap(h.begin(), h.end());
+          } else if (key < h.front()) {
+            std::pop_heap(h.begin(), h.end());
+            h.back() = key;
+            std::push_heap(h.begin(), h.end());
+          }
+        }
+      }
+    }
+    for (uint64_t q = q0; q < q1; ++q) {
+      std::vector<uint64_t>& h = heap[q - q0];
+      std::sort(h.begin(), h.end());
+      for (uint64_t c = 0; c < kp; ++c) {
+        idx[q * kp + c] = static_cast<uint32_t>(h[c] & 0xFFFFFFFFu);
+        const uint32_t key = static_cast<uint32_t>(h[c] >> 32);
+        const uint32_t u = (key & 0x80000000u) ? (key & 0x7FFFFFFFu) : ~key;
+        float f;
+        std::memcpy(&f, &u, 4);
+        dist[q * kp + c] = f;
+      }
+    }
+  }
+  return ORC_OK;
+}
+
 // knn.rs:149-191 restated literally: all n(n-1)/2 upper-triangle triples, one global sort by
 // (distance, i, j), rows filled first come first served. Small n only (O(n^2) memory).
 int orc_knn_exact_allpairs(const float* x, uint64_t n, uint64_t d, uint64_t k, uint32_t* idx, float* dist) {

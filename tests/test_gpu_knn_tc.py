@@ -66,41 +66,56 @@ def test_tc_knn_quantised_ties(lib, orc):
     assert np.array_equal(gd, ed) and np.array_equal(gi, ei)
 
 
-def _tc_vs_simt(lib, x, k):
-    # the tensor-core path (AUTO at n >= 16384) against the exact SIMT path (mode 3), which the tests
-    # above and tests/test_gpu_parity.py pin to the oracle: indices and f32 distances bit-exact
-    gi, gd = lib.knn.find_k_nearest_neighbors(x, k, knn_mode=AUTO)
-    si, sd = lib.knn.find_k_nearest_neighbors(x, k, knn_mode=3)
-    assert np.array_equal(gd, sd)
-    assert np.array_equal(gi, si)
+def _sampled_rows_vs_oracle(lib, orc, x, k, n_rows, seed=0, knn_mode=AUTO):
+    """The GPU's full kNN (AUTO: the tensor-core path at n >= 16384) against the oracle on a seeded sample
+    of query rows (knn.rs:137-194 restated row by row): indices and f32 distances bit-exact."""
+    gi, gd = lib.knn.find_k_nearest_neighbors(x, k, knn_mode=knn_mode)
+    n = x.shape[0]
+    rows = np.sort(np.random.default_rng(seed).choice(n, size=min(n_rows, n), replace=False)).astype(np.uint32)
+    ei, ed = orc.knn_rows(x, rows, k)
+    bad = np.nonzero(~(np.all(gi[rows] == ei, axis=1) & np.all(gd[rows] == ed, axis=1)))[0]
+    assert bad.size == 0, f"{bad.size} of {rows.size} sampled rows differ, first row {rows[bad[0]]}"
+    return gi, gd
 
 
-def test_tc_knn_anisotropic_100k_slice(lib):
-    # a 100,000-row slice of the 1M x 128 generator, preprocessed, k' = 90: the tensor-core filter against
-    # the exact SIMT path
+def test_tc_knn_anisotropic_100k_slice(lib, orc):
+    # a 100,000-row slice of the 1M x 128 generator, preprocessed, k' = 90: 2,000 sampled rows
     from pacmap_b200 import datasets
 
     x, _ = datasets.anisotropic_mixture(n=100000, d=128, k=50, seed=0, draw_seed=5)
     xp = lib.stages.preprocess(x)[0]
-    _tc_vs_simt(lib, xp, 90)
+    _sampled_rows_vs_oracle(lib, orc, xp, 90, 2000)
 
 
-def test_tc_knn_image_like_60k_x_784(lib):
-    # the 60,000 x 784 image-like configuration (quantised to 1/255, many ties), k' = 22 + 50
+def test_tc_knn_image_like_60k_x_784(lib, orc):
+    # the 60,000 x 784 image-like configuration (quantised to 1/255, many ties), k' = 22 + 50: 5,000 rows
     from pacmap_b200 import datasets
 
     x, _ = datasets.image_like(n=60000, d=784, seed=0)
     xp = lib.stages.preprocess(x)[0]
-    _tc_vs_simt(lib, xp, 72)
+    _sampled_rows_vs_oracle(lib, orc, xp, 72, 5000)
 
 
-def test_tc_knn_subspace_mixture_slice_256(lib):
-    # a 100,000-row draw of the 4M x 256 subspace-mixture generator, k' = 49 + 50
+def test_tc_knn_subspace_mixture_slice_256(lib, orc):
+    # a 100,000-row draw of the 4M x 256 subspace-mixture generator, k' = 49 + 50: 2,000 rows
     from pacmap_b200 import datasets
 
     x, _ = datasets.subspace_mixture(n=100000, d=256, seed=2)
     xp = lib.stages.preprocess(x)[0]
-    _tc_vs_simt(lib, xp, 99)
+    _sampled_rows_vs_oracle(lib, orc, xp, 99, 2000)
+
+
+def test_tc_knn_full_1m_x_128(lib, orc):
+    # the benchmarked size: a full 1,000,000 x 128 draw of its generator, preprocessed, k' = 40 + 50,
+    # AUTO mode; 600 sampled rows against the oracle
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.anisotropic_mixture(n=1_000_000, d=128, k=50, seed=0, draw_seed=1000)
+    xp = lib.stages.preprocess(x)[0]
+    gi, gd = _sampled_rows_vs_oracle(lib, orc, xp, 90, 600, seed=1)
+    # size-independent properties over every row: ascending distances, no self, indices in range
+    assert (np.diff(gd, axis=1) >= 0).all()
+    assert (gi < x.shape[0]).all() and not (gi == np.arange(x.shape[0], dtype=np.uint32)[:, None]).any()
 
 
 def test_simt_knn_key_slices(lib, orc):

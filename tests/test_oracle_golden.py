@@ -80,6 +80,19 @@ def test_knn_per_row_equals_reference_allpairs(orc):
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
+def test_knn_rows_equals_full_matrix_rows(orc):
+    # The sampled-row oracle (used at sizes where the full matrix is too slow) returns exactly the rows
+    # of the full per-row oracle, ties included; the allpairs test above pins that one to knn.rs.
+    x, _ = gaussian_mixture(5000, 37, seed=4)
+    x[100:140] = x[7]
+    x = np.round(x, 1).astype(np.float32)
+    rows = np.array([0, 7, 100, 139, 140, 2047, 2048, 4999, 3333, 120], np.uint32)
+    for k in (1, 90, 4999, 6000):
+        full = orc.knn_exact(x, k)
+        got = orc.knn_rows(x, rows, k)
+        assert np.array_equal(got[0], full[0][rows]) and np.array_equal(got[1], full[1][rows])
+
+
 def test_distance_properties(orc):
     # distance.rs:192-268 quickcheck properties: non-negative, zero when equal, symmetric, and equal to
     # the serial sum within f32::EPSILON absolute.
