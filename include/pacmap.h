@@ -68,17 +68,22 @@ typedef enum pacmap_pair_kind {
   PACMAP_PAIRS_ALL_PROVIDED = 2         /* pair_neighbors, pair_mn, pair_fp: rows x 2 each          */
 } pacmap_pair_kind;
 
-/* How the exact kNN is computed (no reference analogue; every mode returns the same indices). */
+/* How the kNN is computed (no reference analogue). Modes 0-3 and 5 return identical exact indices and
+ * distances; mode 4 is approximate from approx_threshold rows on. From 32,768 rows the tensor-core modes
+ * (0-2) skip the column tiles that provably hold no neighbour of a row block (a triangle-inequality
+ * bound through pivot points against a first pass's neighbour-distance bound); mode 5 computes every
+ * tile. */
 typedef enum pacmap_knn_mode {
   PACMAP_KNN_AUTO = 0,         /* tensor-core filter when the dimension allows it, else SIMT exact   */
   PACMAP_KNN_TENSOR_F16 = 1,   /* tcgen05 FP16 distance GEMM filter + exact FP32 re-rank            */
   PACMAP_KNN_TENSOR_BF16 = 2,  /* tcgen05 BF16 distance GEMM filter + exact FP32 re-rank            */
   PACMAP_KNN_SIMT_EXACT = 3,   /* every distance in the reference's FP32 order on CUDA cores        */
-  PACMAP_KNN_APPROX = 4        /* approximate at n >= approx_threshold (the reference's rule,
+  PACMAP_KNN_APPROX = 4,       /* approximate at n >= approx_threshold (the reference's rule,
                                 * src/neighbors.rs:71): each row block searches only the 16 of 256
                                 * pivot cells nearest its own; returned distances stay exact. Below
                                 * the threshold (or below 16,384 rows, where the SIMT path runs) exact;
                                 * pacmap_knn_exact has no threshold: approximate whenever it can be. */
+  PACMAP_KNN_TENSOR_F16_FULL = 5  /* as TENSOR_F16 with every column tile computed (no pruning)     */
 } pacmap_knn_mode;
 
 /* The distance the pairs are drawn with (no reference analogue: the reference is Euclidean only,
@@ -115,7 +120,7 @@ typedef struct pacmap_config {
   uint64_t num_iters[3];               /* default (100, 100, 250)                                    */
   const uint64_t* snapshots;           /* Option<Vec<usize>>: NULL = None                            */
   uint64_t n_snapshots;
-  uint64_t approx_threshold;           /* default 8000; accepted, the engine's kNN is always exact   */
+  uint64_t approx_threshold;           /* default 8000; used by knn_mode APPROX only (else exact)    */
   /* --- engine switches (no reference analogue) --- */
   int32_t knn_mode;                    /* pacmap_knn_mode, default AUTO                              */
   int32_t device;                      /* CUDA device ordinal, default 0                             */
@@ -286,8 +291,9 @@ pacmap_status pacmap_preprocess_noalloc(const float* d_x, uint64_t n, uint64_t d
 /* Stage timing (diagnostics): when enabled, each fit_transform records the device time of its stages
  * with CUDA events on its stream. pacmap_stage_times fills up to `cap` values in milliseconds, in the
  * order preprocess, knn, reselect, sample_mn, sample_fp, csr, init, optimize (then, when the tensor-core
- * kNN ran: its filter kernel alone, and the number of rows it left to the exact fallback), and returns
- * how many. */
+ * kNN ran: its filter kernel alone, the number of rows it left to the exact fallback, the time of the
+ * tile pruning's bound pass and lists, and the (row block, column tile) pairs computed, of the full
+ * sweep, and of the bound pass), and returns how many. */
 void pacmap_set_stage_timing(int32_t enabled);
 uint64_t pacmap_stage_times(double* out_ms, uint64_t cap);
 

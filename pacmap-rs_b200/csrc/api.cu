@@ -180,14 +180,18 @@ void generate_pairs_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, co
   DevBuf<uint32_t> idx(c, n * kp);
   DevBuf<float> dist(c, n * kp), sig(c, n);
   if (tm) tm->start(ST_KNN);
-  last_tc_filter_ms() = 0.0;
-  last_tc_fallback_rows() = 0;
+  last_tc_stats() = KnnTcStats();
   knn_exact_device(c, d_xp, n, d, kp, knn_mode, idx.get(), dist.get(), KnnShard(), approx_threshold);
   if (tm) tm->stop(ST_KNN);
   if (tm && tm->on) {
-    g_stage_ms.resize(ST_COUNT + 2, 0.0);
-    g_stage_ms[ST_COUNT] = last_tc_filter_ms();
-    g_stage_ms[ST_COUNT + 1] = static_cast<double>(last_tc_fallback_rows());
+    const KnnTcStats& ks = last_tc_stats();
+    g_stage_ms.resize(ST_COUNT + 6, 0.0);
+    g_stage_ms[ST_COUNT] = ks.filter_ms;
+    g_stage_ms[ST_COUNT + 1] = static_cast<double>(ks.fallback_rows);
+    g_stage_ms[ST_COUNT + 2] = ks.bound_ms;
+    g_stage_ms[ST_COUNT + 3] = static_cast<double>(ks.tiles_visited);
+    g_stage_ms[ST_COUNT + 4] = static_cast<double>(ks.tiles_full);
+    g_stage_ms[ST_COUNT + 5] = static_cast<double>(ks.tiles_bound);
   }
   if (tm) tm->start(ST_RESELECT);
   sigma_device(c, dist.get(), n, kp, sig.get());
@@ -212,7 +216,7 @@ void validate_config(const pacmap_config* cfg) {
   PM_REQUIRE(cfg != nullptr, PACMAP_ERR_INVALID_ARGUMENT, "config is NULL");
   PM_REQUIRE(cfg->init_kind >= 0 && cfg->init_kind <= 2, PACMAP_ERR_INVALID_ARGUMENT, "unknown init_kind");
   PM_REQUIRE(cfg->pair_kind >= 0 && cfg->pair_kind <= 2, PACMAP_ERR_INVALID_ARGUMENT, "unknown pair_kind");
-  PM_REQUIRE(cfg->knn_mode >= 0 && cfg->knn_mode <= 4, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
+  PM_REQUIRE(cfg->knn_mode >= 0 && cfg->knn_mode <= 5, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
   PM_REQUIRE(cfg->metric == PACMAP_METRIC_EUCLIDEAN || cfg->metric == PACMAP_METRIC_ANGULAR,
              PACMAP_ERR_INVALID_ARGUMENT, "unknown metric");
 }
@@ -585,7 +589,7 @@ pacmap_status pacmap_knn_exact(const float* x, uint64_t n, uint64_t d, uint64_t 
     const uint64_t kp = std::min<uint64_t>(k, n - 1);
     if (kp == 0) return;
     PM_REQUIRE(x && out_idx && out_dist, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
-    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 4, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
+    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 5, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
     DeviceLock dl(device);
     Ctx& c = dl.ctx;
     DevBuf<float> dx, dd(c, n * kp);
@@ -607,7 +611,7 @@ pacmap_status pacmap_knn_exact_shard(const float* x, uint64_t n, uint64_t d, uin
     if (n == 0) return;
     const uint64_t kp = std::min<uint64_t>(k, n - 1);
     PM_REQUIRE(x && out_owned && (kp == 0 || (out_idx && out_dist)), PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
-    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 4, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
+    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 5, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
     DeviceLock dl(device);
     Ctx& c = dl.ctx;
     DevBuf<float> dx, dd(c, n * kp);

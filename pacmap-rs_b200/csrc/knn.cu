@@ -233,10 +233,12 @@ void knn_exact_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t
   PM_REQUIRE(shard.count >= 1 && shard.index < shard.count, PACMAP_ERR_INVALID_ARGUMENT, "bad kNN shard");
   // AUTO uses the tensor cores once the O(n^2) part dominates; the TENSOR modes force them.
   const bool approx = mode == PACMAP_KNN_APPROX && n >= approx_threshold;
-  const bool want_tc = (mode == PACMAP_KNN_TENSOR_F16 || mode == PACMAP_KNN_TENSOR_BF16) ||
+  const bool want_tc = (mode == PACMAP_KNN_TENSOR_F16 || mode == PACMAP_KNN_TENSOR_BF16 ||
+                        mode == PACMAP_KNN_TENSOR_F16_FULL) ||
                        ((mode == PACMAP_KNN_AUTO || mode == PACMAP_KNN_APPROX) && n >= 16384);
   if (want_tc && knn_tc_supported(n, d, kp)) {
-    if (knn_tc_device(c, d_x, n, d, kp, mode == PACMAP_KNN_TENSOR_BF16, d_idx, d_dist, shard, approx ? 16 : 0))
+    if (knn_tc_device(c, d_x, n, d, kp, mode == PACMAP_KNN_TENSOR_BF16, d_idx, d_dist, shard, approx ? 16 : 0,
+                      /*prune=*/mode != PACMAP_KNN_TENSOR_F16_FULL))
       return;
   }
   PM_REQUIRE(mode == PACMAP_KNN_AUTO || mode == PACMAP_KNN_SIMT_EXACT || mode == PACMAP_KNN_APPROX,

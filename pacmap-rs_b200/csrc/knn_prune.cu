@@ -1,0 +1,385 @@
+// Pivots of the locality order, and certified tile pruning for the exact tensor-core kNN.
+//
+// The filter (knn_tc.cu) runs the distance GEMM of every (row block of 256, column tile of 128) pair of
+// the locality order. Most pairs cannot hold a neighbour. Through any pivot p the triangle inequality
+// bounds a distance from below, |x_i - x_j| >= | |x_i - p| - |x_j - p| |, so for a row segment s and a
+// column segment t (the rows of one pivot cell inside one tile):
+//     min over i in s, j in t of |x_i - x_j|  >=  LB(s, t) = max( m_s(p_t) - R_t, m_t(p_s) - R_s ),
+// with p_s the pivot of s's cell, R_s = max_{i in s} |x_i - p_s| (the segment's radius) and
+// m_s(p) = min_{i in s} |x_i - p|. A first filter pass over the cells nearest each block gives every
+// row i an upper bound U_i of its k'-th neighbour distance (any k' other points give one). A column tile
+// is skipped for a row block when LB(s, t) > max_{i in s} U_i for every row segment s of the block and
+// every segment t of the tile: no point of the tile can be among the k' nearest of any of the block's
+// rows, ties included. The kept tiles go through the unchanged filter, whose candidate sets stay
+// complete, so the exact re-rank returns the reference's rows (src/knn.rs:137-194) bit for bit.
+// Every bound is widened for its f32 rounding: the pivot distances by an explicit error term, and the
+// final comparison by a relative margin of 1e-4 that also covers the reference's own f32 distance sum.
+//
+// Pivots: k-means++ seeding (Arthur & Vassilvitskii, SODA 2007) in batches of 16 draws on a subsample of
+// at most 65,536 rows, so that every well-separated group of points receives a pivot and the cells stay
+// compact; the draws come from a Philox4x32-10 stream with a fixed key (the same pivots on every call).
+#include <algorithm>
+#include <cmath>
+
+#include "knn_layout.cuh"
+#include "knn_prune.cuh"
+
+namespace pacmap {
+
+namespace {
+
+constexpr int PV_BATCH = 16;             // pivots drawn per round
+constexpr uint32_t PV_SUB_MAX = 65536;   // subsample size limit
+constexpr int PV_CHUNK = 256;            // subsample points per block (and per prefix-sum entry)
+constexpr uint32_t TAG_PIVOT = 0x50495654u;  // 'PIVT'
+constexpr int SEGS = 4;                  // cell segments kept per tile (further cells merge into the last)
+constexpr float PRUNE_MARGIN = 1e-4f;    // relative margin of the skip test
+
+__host__ __device__ __forceinline__ uint64_t sub_row(uint32_t s, uint32_t S, uint64_t n) {
+  return static_cast<uint64_t>(s) * n / S;
+}
+
+// dmin[s] = min(dmin[s], |x_row(s) - q|^2 over the 16 pivots q of the batch starting at p0) for the
+// subsample points of this block's chunk, and the chunk's sum of dmin (f64, a fixed order). p0 == 0
+// starts dmin from +inf. One warp per point, lanes over the columns; the batch is staged in shared memory.
+__global__ void __launch_bounds__(256) pivot_dmin_kernel(const float* __restrict__ x, uint64_t n, int d, uint32_t S,
+                                                         const uint32_t* __restrict__ piv_rows, int p0,
+                                                         float* __restrict__ dmin, double* __restrict__ chunk_sum) {
+  extern __shared__ float pv[];  // PV_BATCH x d
+  __shared__ double wsum[8];
+  for (int e = threadIdx.x; e < PV_BATCH * d; e += blockDim.x) {
+    const int q = e / d, col = e - q * d;
+    pv[e] = x[static_cast<uint64_t>(piv_rows[p0 + q]) * d + col];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int PER_WARP = PV_CHUNK / 8;
+  double ws = 0.0;
+  for (int t = 0; t < PER_WARP; ++t) {
+    const uint32_t s = blockIdx.x * PV_CHUNK + warp * PER_WARP + t;
+    if (s >= S) break;  // warp-uniform
+    const float* xr = x + sub_row(s, S, n) * d;
+    float acc[PV_BATCH];
+#pragma unroll
+    for (int q = 0; q < PV_BATCH; ++q) acc[q] = 0.0f;
+    for (int col = lane; col < d; col += 32) {
+      const float xv = xr[col];
+#pragma unroll
+      for (int q = 0; q < PV_BATCH; ++q) {
+        const float df = xv - pv[q * d + col];
+        acc[q] = fmaf(df, df, acc[q]);
+      }
+    }
+    float best = p0 == 0 ? __int_as_float(0x7f800000) : dmin[s];
+#pragma unroll
+    for (int q = 0; q < PV_BATCH; ++q) {
+      float v = acc[q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);  // the same sum on every lane
+      best = fminf(best, v);
+    }
+    if (lane == 0) dmin[s] = best;
+    if (best < 3.0e38f) ws += static_cast<double>(best);
+  }
+  if (lane == 0) wsum[warp] = ws;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double total = 0.0;
+    for (int w = 0; w < 8; ++w) total += wsum[w];
+    chunk_sum[blockIdx.x] = total;
+  }
+}
+
+// Round 0: 16 evenly spaced subsample points. Round r > 0: 16 draws, each point with probability
+// proportional to dmin (its squared distance to the nearest pivot so far); a degenerate subsample (all
+// dmin zero) falls back to evenly spaced points.
+__global__ void __launch_bounds__(64) pivot_draw_kernel(const float* __restrict__ dmin, uint32_t S, uint64_t n,
+                                                        const double* __restrict__ chunk_sum, int nchunks, int round,
+                                                        uint32_t* __restrict__ piv_rows) {
+  __shared__ double pre[PV_SUB_MAX / PV_CHUNK + 1];
+  if (threadIdx.x == 0) {
+    double run = 0.0;
+    pre[0] = 0.0;
+    for (int ch = 0; round > 0 && ch < nchunks; ++ch) {
+      const double v = chunk_sum[ch];
+      run += (v > 0.0 && v < 1e300) ? v : 0.0;
+      pre[ch + 1] = run;
+    }
+  }
+  __syncthreads();
+  const int b = threadIdx.x;
+  if (b >= PV_BATCH) return;
+  uint32_t s = round == 0 ? static_cast<uint32_t>(static_cast<uint64_t>(b) * S / PV_BATCH)
+                          : static_cast<uint32_t>(static_cast<uint64_t>(round * PV_BATCH + b) * S / PIV);
+  const double total = round > 0 ? pre[nchunks] : 0.0;
+  if (round > 0 && total > 0.0 && total < 1e300) {
+    uint32_t w[4];
+    philox4x32_10(static_cast<uint32_t>(round), static_cast<uint32_t>(b), 0u, TAG_PIVOT, 0x9E3779B9u, 0x7F4A7C15u, w);
+    const uint64_t bits53 = (static_cast<uint64_t>(w[0]) << 21) | (w[1] >> 11);
+    const double target = static_cast<double>(bits53) * (1.0 / 9007199254740992.0) * total;
+    int lo = 0, hi = nchunks - 1;  // the last chunk whose prefix is <= target
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pre[mid] <= target) lo = mid;
+      else hi = mid - 1;
+    }
+    double acc = pre[lo];
+    const uint32_t a = static_cast<uint32_t>(lo) * PV_CHUNK, e = min(S, a + PV_CHUNK);
+    uint32_t pick = 0xFFFFFFFFu;
+    for (uint32_t t = a; t < e; ++t) {
+      const float v = dmin[t];
+      if (v > 0.0f && v < 3.0e38f) {
+        pick = t;
+        acc += v;
+        if (acc > target) break;
+      }
+    }
+    if (pick != 0xFFFFFFFFu) s = pick;
+  }
+  piv_rows[round * PV_BATCH + b] = static_cast<uint32_t>(sub_row(s, S, n));
+}
+
+// Per column tile (128 positions): its rows split by pivot cell into at most SEGS segments (cells are
+// contiguous in the locality order; cells past the fourth merge into the fourth, whose pivot stays its
+// first cell's). Per segment g: seg_cell, the radius seg_rad = max |x_i - p_cell| (rounded up), the
+// largest row bound seg_ub = max U_i, and for every pivot p, minT[p * nseg + g] = min |x_i - p| (rounded
+// down). One thread per pivot; a non-finite distance or bound makes the segment unprunable (-inf / +inf).
+__global__ void __launch_bounds__(PIV) seg_stats_kernel(PruneInputs in, float errc, int* __restrict__ seg_cell,
+                                                        float* __restrict__ seg_rad, float* __restrict__ seg_ub,
+                                                        float* __restrict__ minT, uint64_t nseg) {
+  __shared__ float rad_s[SEGS];
+  const uint64_t tile = blockIdx.x;
+  const uint64_t r0 = tile * TC_BN, r1 = min(r0 + TC_BN, in.n);
+  const int p = threadIdx.x;
+  const float inf = __int_as_float(0x7f800000);
+  const float inv_s2 = in.inv_s * in.inv_s;
+  float mn[SEGS], rad[SEGS], ubm[SEGS];
+  int cl[SEGS];
+#pragma unroll
+  for (int q = 0; q < SEGS; ++q) {
+    mn[q] = inf;
+    rad[q] = 0.0f;
+    ubm[q] = 0.0f;
+    cl[q] = -1;
+  }
+  const float pn = in.pnorm[p];
+  int s = -1;
+  uint32_t prev = 0xFFFFFFFFu;
+  for (uint64_t r = r0; r < r1; ++r) {
+    const uint32_t o = in.perm[r];
+    const uint32_t cc = in.cell[o];
+    if (cc != prev) {
+      prev = cc;
+      if (s < SEGS - 1) {
+        ++s;
+#pragma unroll
+        for (int q = 0; q < SEGS; ++q)
+          if (q == s) cl[q] = static_cast<int>(cc);
+      }
+    }
+    const float xn = in.rownorm[r] * inv_s2;  // |x|^2: the scale is an exact power of two
+    const float d2 = in.score[static_cast<uint64_t>(o) * PIV + p] + xn;
+    const float err = errc * (xn + pn);
+    float lo = sqrtf(fmaxf(d2 - err, 0.0f)) * (1.0f - 2.4e-7f);
+    if (!(lo >= 0.0f)) lo = -inf;  // NaN
+    float hi = sqrtf(d2 + err) * (1.0f + 2.4e-7f);
+    if (!(hi <= 3.4e38f)) hi = inf;
+    float u = 0.0f;
+    if (p == 0) {
+      const float ub = in.ub[r];
+      u = ub >= 0.0f ? sqrtf(ub) * in.inv_s * (1.0f + 4.8e-7f) : inf;
+      if (!(u <= 3.4e38f)) u = inf;
+    }
+#pragma unroll
+    for (int q = 0; q < SEGS; ++q) {
+      if (q == s) {
+        mn[q] = fminf(mn[q], lo);
+        if (p == cl[q]) rad[q] = fmaxf(rad[q], hi);
+        if (p == 0) ubm[q] = fmaxf(ubm[q], u);
+      }
+    }
+  }
+  // each segment's radius lives in the thread of its pivot
+#pragma unroll
+  for (int q = 0; q < SEGS; ++q)
+    if (cl[q] == p) rad_s[q] = rad[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < SEGS; ++q) minT[static_cast<uint64_t>(p) * nseg + tile * SEGS + q] = mn[q];
+  if (p == 0) {
+#pragma unroll
+    for (int q = 0; q < SEGS; ++q) {
+      seg_cell[tile * SEGS + q] = cl[q];
+      seg_rad[tile * SEGS + q] = cl[q] >= 0 ? rad_s[q] : 0.0f;
+      seg_ub[tile * SEGS + q] = ubm[q];
+    }
+  }
+}
+
+// One block per row block: the visit bit of every column tile and the count of visited tiles. The
+// block's row segments are those of its two tiles; a tile is visited unless every (row segment, tile
+// segment) pair is separated by more than the row segment's bound. The block's own tiles are always kept.
+__global__ void __launch_bounds__(256) prune_tiles_kernel(const int* __restrict__ seg_cell,
+                                                          const float* __restrict__ seg_rad,
+                                                          const float* __restrict__ seg_ub,
+                                                          const float* __restrict__ minT, uint64_t nseg, int ntiles,
+                                                          int words, int blk0, uint32_t* __restrict__ bits,
+                                                          uint32_t* __restrict__ counts) {
+  __shared__ float ms[2 * SEGS][PIV];
+  __shared__ int sp[2 * SEGS];
+  __shared__ float srad[2 * SEGS], sthr[2 * SEGS];
+  __shared__ uint32_t wcount[8];
+  const int blk = static_cast<int>(blockIdx.x) + blk0;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint64_t g0 = static_cast<uint64_t>(2 * blk) * SEGS;
+  if (tid < 2 * SEGS) {
+    const int cl = seg_cell[g0 + tid];
+    sp[tid] = cl;
+    srad[tid] = cl >= 0 ? seg_rad[g0 + tid] : 0.0f;
+    sthr[tid] = cl >= 0 ? seg_ub[g0 + tid] * (1.0f + PRUNE_MARGIN) : 0.0f;
+  }
+  __syncthreads();
+  for (int q = 0; q < 2 * SEGS; ++q) ms[q][tid] = sp[q] >= 0 ? minT[static_cast<uint64_t>(tid) * nseg + g0 + q] : 0.0f;
+  __syncthreads();
+  uint32_t cnt = 0;
+  for (int base = 0; base < ntiles; base += 256) {
+    const int J = base + tid;
+    bool visit = false;
+    if (J < ntiles) {
+      visit = (J >> 1) == blk;
+      for (int qt = 0; qt < SEGS && !visit; ++qt) {
+        const uint64_t t = static_cast<uint64_t>(J) * SEGS + qt;
+        const int pt = seg_cell[t];
+        if (pt < 0) break;  // segments are filled in order
+        const float rt = seg_rad[t];
+        for (int qs = 0; qs < 2 * SEGS; ++qs) {
+          const int ps = sp[qs];
+          if (ps < 0) continue;
+          const float lb = fmaxf(ms[qs][pt] - rt, minT[static_cast<uint64_t>(ps) * nseg + t] - srad[qs]);
+          if (!(lb * (1.0f - PRUNE_MARGIN) > sthr[qs])) {
+            visit = true;
+            break;
+          }
+        }
+      }
+    }
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, visit);
+    const int word = (base >> 5) + warp;
+    if (lane == 0 && word < words) {
+      bits[static_cast<uint64_t>(blk) * words + word] = bal;
+      cnt += __popc(bal);
+    }
+  }
+  if (lane == 0) wcount[warp] = cnt;
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t total = 0;
+    for (int w = 0; w < 8; ++w) total += wcount[w];
+    counts[blk] = total;
+  }
+}
+
+// ptr[b] = sum of counts[0..b), ptr[nb] the total (one block).
+__global__ void __launch_bounds__(1024) scan_counts_kernel(const uint32_t* __restrict__ counts, uint64_t nb,
+                                                           uint32_t* __restrict__ ptr) {
+  __shared__ uint32_t part[1024];
+  const uint64_t per = (nb + 1023) / 1024;
+  const uint64_t a = threadIdx.x * per, e = min(nb, a + per);
+  uint32_t s = 0;
+  for (uint64_t i = a; i < e; ++i) s += counts[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const uint32_t v = threadIdx.x >= static_cast<unsigned>(o) ? part[threadIdx.x - o] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
+  for (uint64_t i = a; i < e; ++i) {
+    ptr[i] = run;
+    run += counts[i];
+  }
+  if (threadIdx.x == 1023) ptr[nb] = part[1023];
+}
+
+// One warp per row block: its visited tiles in the sweep order (the window around its own rows first).
+__global__ void __launch_bounds__(128) fill_tile_lists_kernel(const uint32_t* __restrict__ bits, int words, int ntiles,
+                                                              const uint32_t* __restrict__ ptr, int blk0, int nblk,
+                                                              uint32_t* __restrict__ list) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = static_cast<int>(blockIdx.x) * 4 + warp;
+  if (j >= nblk) return;
+  const int blk = blk0 + j;
+  uint32_t pos = ptr[blk];
+  for (int t0 = 0; t0 < ntiles; t0 += 32) {
+    const int t = t0 + lane;
+    bool v = false;
+    int tile = 0;
+    if (t < ntiles) {
+      tile = sweep_tile(t, blk, ntiles);
+      v = (bits[static_cast<uint64_t>(blk) * words + (tile >> 5)] >> (tile & 31)) & 1u;
+    }
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, v);
+    if (v) list[pos + __popc(bal & ((1u << lane) - 1u))] = static_cast<uint32_t>(tile);
+    pos += __popc(bal);
+  }
+}
+
+}  // namespace
+
+void select_pivots(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint32_t* d_piv_rows) {
+  const uint32_t S = static_cast<uint32_t>(std::min<uint64_t>(n, PV_SUB_MAX));
+  const int nchunks = static_cast<int>(ceil_div(S, PV_CHUNK));
+  DevBuf<float> dmin(c, S);
+  DevBuf<double> csum(c, nchunks);
+  const size_t smem = static_cast<size_t>(PV_BATCH) * d * sizeof(float);
+  PM_CUDA(cudaFuncSetAttribute(pivot_dmin_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  pivot_draw_kernel<<<1, 64, 0, c.stream>>>(dmin.get(), S, n, csum.get(), nchunks, 0, d_piv_rows);
+  PM_LAUNCHED();
+  for (int r = 1; r < PIV / PV_BATCH; ++r) {
+    pivot_dmin_kernel<<<nchunks, 256, smem, c.stream>>>(d_x, n, static_cast<int>(d), S, d_piv_rows, (r - 1) * PV_BATCH,
+                                                        dmin.get(), csum.get());
+    PM_LAUNCHED();
+    pivot_draw_kernel<<<1, 64, 0, c.stream>>>(dmin.get(), S, n, csum.get(), nchunks, r, d_piv_rows);
+    PM_LAUNCHED();
+  }
+}
+
+uint64_t build_pruned_tile_lists(Ctx& c, const PruneInputs& in, DevBuf<uint32_t>& ptr, DevBuf<uint32_t>& list) {
+  const uint64_t nb = in.n_pad / TC_BM, ntiles = in.n_pad / TC_BN;
+  const uint64_t nseg = ntiles * SEGS;
+  const int words = static_cast<int>((ntiles + 31) / 32);
+  DevBuf<int> seg_cell(c, nseg);
+  DevBuf<float> seg_rad(c, nseg), seg_ub(c, nseg), minT(c, static_cast<uint64_t>(PIV) * nseg);
+  // |p|^2 - 2 x.p + |x|^2 with fused multiply-add sums over d terms: within (3d + 16) 2^-24 (|x|^2 + |p|^2)
+  const float errc = static_cast<float>(3 * in.d + 16) * 5.9604644775390625e-08f;
+  seg_stats_kernel<<<static_cast<unsigned>(ntiles), PIV, 0, c.stream>>>(in, errc, seg_cell.get(), seg_rad.get(),
+                                                                         seg_ub.get(), minT.get(), nseg);
+  PM_LAUNCHED();
+  DevBuf<uint32_t> bits(c, nb * words), counts(c, nb);
+  PM_CUDA(cudaMemsetAsync(counts.get(), 0, nb * sizeof(uint32_t), c.stream));
+  const unsigned nblk = static_cast<unsigned>(in.blk1 - in.blk0);
+  if (nblk) {
+    prune_tiles_kernel<<<nblk, 256, 0, c.stream>>>(seg_cell.get(), seg_rad.get(), seg_ub.get(), minT.get(), nseg,
+                                                   static_cast<int>(ntiles), words, static_cast<int>(in.blk0),
+                                                   bits.get(), counts.get());
+    PM_LAUNCHED();
+  }
+  ptr.alloc(c, nb + 1);
+  scan_counts_kernel<<<1, 1024, 0, c.stream>>>(counts.get(), nb, ptr.get());
+  PM_LAUNCHED();
+  uint32_t total = 0;
+  PM_CUDA(cudaMemcpyAsync(&total, ptr.get() + nb, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+  PM_CUDA(cudaStreamSynchronize(c.stream));
+  list.alloc(c, std::max<uint64_t>(total, 1));
+  if (nblk) {
+    fill_tile_lists_kernel<<<ceil_div(nblk, 4), 128, 0, c.stream>>>(bits.get(), words, static_cast<int>(ntiles),
+                                                                    ptr.get(), static_cast<int>(in.blk0),
+                                                                    static_cast<int>(nblk), list.get());
+    PM_LAUNCHED();
+  }
+  return total;
+}
+
+}  // namespace pacmap

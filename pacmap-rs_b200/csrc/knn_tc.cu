@@ -34,6 +34,8 @@
 #include <string>
 #include <vector>
 
+#include "knn_layout.cuh"
+#include "knn_prune.cuh"
 #include "knn_tc.cuh"
 #include "ptx.cuh"
 #include "tcgen05.cuh"
@@ -42,8 +44,6 @@ namespace pacmap {
 
 namespace {
 
-constexpr int TC_BM = 256;         // rows per block (two M = 128 accumulators)
-constexpr int TC_BN = 128;         // columns per tile (MMA N)
 constexpr int TC_MAX_STAGES = 8;   // operand pipeline depth limit (mbarrier slots)
 constexpr int TC_THREADS = 320;    // warp 0 TMA, warp 1 MMA + TMEM owner, warps 2..9 epilogue
 constexpr int TC_EPI_WARPS = 8;
@@ -70,6 +70,8 @@ struct alignas(8) TcShared {
 //              tile (A is re-read from L2 for every tile). KB is a run-time value here.
 // The column-term tile rides with the first stage of each column tile.
 enum FilterMode { MODE_TILE = 0, MODE_KBLOCK = 1, MODE_STREAM = 2 };
+constexpr uint64_t PRUNE_MIN_ROWS = 32768;  // tile pruning from 256 column tiles on
+constexpr int PRUNE_PROBE = 2;              // cells per row block in the pruning's bound pass (own + nearest)
 constexpr int TC_SMEM_LIMIT = 232448;  // 227 KB of dynamic shared memory per block
 template <int KB, int MODE>
 struct FilterLayout {
@@ -103,7 +105,8 @@ __device__ __forceinline__ float theta_from(uint32_t ukey, float n_i, float e4_i
 // by bisection on the registers, entries with v <= theta survive (order kept) and are written back once.
 template <int PER>
 __device__ __forceinline__ int warp_compact_regs(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
-                                                 const float2* __restrict__ ge, float& theta_out) {
+                                                 const float2* __restrict__ ge, float& theta_out,
+                                                 uint32_t* ukey_out = nullptr) {
   const int lane = threadIdx.x & 31;
   uint32_t ri[PER];
   float rv[PER];
@@ -153,6 +156,7 @@ __device__ __forceinline__ int warp_compact_regs(uint2* __restrict__ cand, int m
   }
   __syncwarp();
   theta_out = th;
+  if (ukey_out) *ukey_out = prefix;
   return out;
 }
 
@@ -193,14 +197,16 @@ __device__ __forceinline__ int warp_compact(uint32_t* __restrict__ idx, float* _
 //    puts near points in near rows, so each row block meets its own neighbourhood first (sweep
 //    order below) and its threshold tightens after a few tiles. Any order gives the same exact kNN.
 // ---------------------------------------------------------------------------------------------
-constexpr int PIV = 256;
-
 // Register-tiled: a block takes 64 points and the pivots in two passes of 128; each thread keeps 4
 // points x 8 pivots of dot products while d is staged through shared memory in slices of 32. Any
-// assignment order gives the same kNN; this one only has to be fast.
+// assignment order gives the same kNN; this one only has to be fast. With `score` (n x PIV) it also
+// stores |p|^2 - 2 x.p of every (point, pivot) pair, and block 0 stores |p|^2 in `pnorm` (the tile
+// pruning's pivot distances).
 constexpr int PA_PTS = 64, PA_PIV = 128, PA_D = 32;
 __global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restrict__ x, uint64_t n, int d,
-                                                           uint32_t* __restrict__ cell) {
+                                                           const uint32_t* __restrict__ piv_rows,
+                                                           uint32_t* __restrict__ cell, float* __restrict__ score,
+                                                           float* __restrict__ pnorm) {
   __shared__ float xs[PA_D][PA_PTS + 4];  // [dim][point]
   __shared__ float ps[PA_D][PA_PIV + 4];  // [dim][pivot]
   __shared__ float pn[PA_PIV];
@@ -227,7 +233,7 @@ __global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restri
       }
       for (int e = threadIdx.x; e < PA_D * PA_PIV; e += 256) {
         const int pv = e / PA_D, cc = e % PA_D;
-        const uint64_t prow = static_cast<uint64_t>(half * PA_PIV + pv) * n / PIV;
+        const uint64_t prow = piv_rows[half * PA_PIV + pv];
         ps[cc][pv] = (c0 + cc < d) ? x[prow * d + c0 + cc] : 0.0f;
       }
       __syncthreads();
@@ -247,20 +253,31 @@ __global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restri
       }
     }
     __syncthreads();
-    if (threadIdx.x < PA_PIV) pn[threadIdx.x] = nrm;
+    if (threadIdx.x < PA_PIV) {
+      pn[threadIdx.x] = nrm;
+      if (pnorm && blockIdx.x == 0) pnorm[half * PA_PIV + threadIdx.x] = nrm;
+    }
     __syncthreads();
     // per point: the best of this thread's 8 pivots, then of the 16 threads sharing the point
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       float b = __int_as_float(0x7f800000);
       uint32_t bi = 0;
+      float sc8[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const float sc = fmaf(-2.0f, acc[i][j], pn[tq * 8 + j]);
+        sc8[j] = sc;
         if (sc < b) {
           b = sc;
           bi = static_cast<uint32_t>(half * PA_PIV + tq * 8 + j);
         }
+      }
+      const uint64_t pt = pt0 + tp * 4 + i;
+      if (score && pt < n) {
+        float4* dst = reinterpret_cast<float4*>(score + pt * PIV + half * PA_PIV + tq * 8);
+        dst[0] = make_float4(sc8[0], sc8[1], sc8[2], sc8[3]);
+        dst[1] = make_float4(sc8[4], sc8[5], sc8[6], sc8[7]);
       }
       best_s[tp * 4 + i][tq] = b;
       best_i[tp * 4 + i][tq] = bi;
@@ -340,19 +357,6 @@ __global__ void __launch_bounds__(32) cell_place_kernel(const uint32_t* __restri
     if (valid && lane == __ffs(same) - 1) off[cl] += __popc(same);
     __syncwarp();
   }
-}
-
-// Column tile visited at step t by row block b: first the window of W tiles around the block's own
-// rows, then every other tile in ascending order (all blocks of a wave advance through the same
-// region, which keeps the B operand in L2).
-constexpr int SWEEP_W = 16;
-__host__ __device__ __forceinline__ int sweep_tile(int t, int b, int ntiles) {
-  if (ntiles <= SWEEP_W) return t;
-  int w0 = 2 * b - SWEEP_W / 2 + 1;
-  w0 = w0 < 0 ? 0 : (w0 > ntiles - SWEEP_W ? ntiles - SWEEP_W : w0);
-  if (t < SWEEP_W) return w0 + t;
-  const int r = t - SWEEP_W;
-  return r < w0 ? r : r + SWEEP_W;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -767,22 +771,39 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
 // ---------------------------------------------------------------------------------------------
 // 3a. final compaction: the row's certified band (v <= theta of its rank-th upper bound), one warp
 //     per row; the count is written back (rows that overflowed in the filter keep -1).
+//     With ub (the tile pruning's first pass): ub[r] = the rank-th smallest upper bound of the reference's
+//     squared distance (scaled by s^2) over the columns the row met, u + n_i + 2 e_i rounded up -- an
+//     upper bound of its k'-th neighbour distance, since k' of those rank columns are other points;
+//     +inf when the row met fewer than rank columns or overflowed.
 constexpr int RC_WARPS = 4;
 
 template <int PER>
 __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     uint64_t n, int rank, const float* __restrict__ nrm, const float2* __restrict__ ge, uint2* __restrict__ cand,
-    int* __restrict__ cand_cnt) {
+    int* __restrict__ cand_cnt, float* __restrict__ ub) {
   constexpr int C = 32 * PER;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * RC_WARPS + warp; r < n;
        r += static_cast<uint64_t>(gridDim.x) * RC_WARPS) {
     const int m0 = min(cand_cnt[r], C);
-    if (m0 <= 0) continue;
+    if (m0 <= 0 || (ub && m0 < rank)) {
+      if (ub && lane == 0) ub[r] = __int_as_float(0x7f800000);
+      continue;
+    }
     const uint64_t rb = r * static_cast<uint64_t>(C);
     float th;
-    const int m = warp_compact_regs<PER>(cand + rb, m0, min(rank, m0), nrm[r], ge[r].y, ge, th);
-    if (lane == 0) cand_cnt[r] = m;
+    uint32_t ukey = 0;
+    const float n_i = nrm[r], e4_i = ge[r].y;
+    const int m = warp_compact_regs<PER>(cand + rb, m0, min(rank, m0), n_i, e4_i, ge, th, &ukey);
+    if (lane == 0) {
+      cand_cnt[r] = m;
+      if (ub) {
+        // two f32 additions: within 2^-23 of the magnitudes summed (rounded up by 2^-22 of them)
+        const float uk = key_to_float(ukey);
+        const float u = (uk + n_i + 0.5f * e4_i) + 2.384185791015625e-07f * (fabsf(uk) + n_i + e4_i);
+        ub[r] = (u >= 0.0f && u <= 3.4e38f) ? u : __int_as_float(0x7f800000);
+      }
+    }
   }
 }
 
@@ -873,10 +894,11 @@ bool knn_tc_supported(uint64_t n, uint64_t d, uint64_t kp) {
   return d >= 1 && d <= 1024 && kp >= 1 && kp + 1 <= 448 && n >= 2 && n < (1ull << 31);
 }
 
-// The pivots' rows (pivot p is point p * n / PIV) into a PIV x d array.
-__global__ void gather_pivots_kernel(const float* __restrict__ x, uint64_t n, int d, float* __restrict__ out) {
+// The pivots' rows into a PIV x d array.
+__global__ void gather_pivots_kernel(const float* __restrict__ x, const uint32_t* __restrict__ piv_rows, int d,
+                                     float* __restrict__ out) {
   const int p = blockIdx.x;
-  const uint64_t row = static_cast<uint64_t>(p) * n / PIV;
+  const uint64_t row = piv_rows[p];
   for (int c = threadIdx.x; c < d; c += blockDim.x) out[static_cast<uint64_t>(p) * d + c] = x[row * d + c];
 }
 
@@ -887,15 +909,20 @@ __global__ void mark_owned_kernel(const uint32_t* __restrict__ perm, uint64_t r0
 }
 
 bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp, bool bf16, uint32_t* d_idx,
-                   float* d_dist, const KnnShard& shard, int nprobe) {
+                   float* d_dist, const KnnShard& shard, int nprobe, bool prune) {
   if (!knn_tc_supported(n, d, kp)) return false;
+  KnnTcStats& st = last_tc_stats();
+  st = KnnTcStats();
   const int KB = static_cast<int>((d + 63) / 64);
   const int KP = 64 * KB;
   const int mode = KB <= 2 ? MODE_TILE : (KB <= 4 ? MODE_KBLOCK : MODE_STREAM);
   const uint64_t n_pad = (n + TC_BM - 1) / TC_BM * TC_BM;
+  const uint64_t nblocks = n_pad / TC_BM, ntl = n_pad / TC_BN;
   const int PER = (kp + 1 <= 192) ? 16 : 32;  // buffer C = 512 or 1024 candidates per row
   const int C = 32 * PER;
   const int rank = static_cast<int>(kp) + 1;
+  // Tile pruning pays once the tiles are many; its lists are indexed with 32 bits.
+  prune = prune && nprobe == 0 && n >= PRUNE_MIN_ROWS && nblocks * ntl < (1ull << 32);
 
   // scale: an exact power of two with max |x s| < 2^13
   DevBuf<uint32_t> amax(c, 1);
@@ -912,10 +939,17 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   std::frexp(amx, &ex);  // amx in [2^(ex-1), 2^ex)
   const float s = std::ldexp(1.0f, 13 - ex);
 
-  // locality order
+  // locality order: pivots by k-means++ seeding, every point to its nearest pivot, a stable sort by cell
   const uint32_t chunks = ceil_div(n, PL_CHUNK);
-  DevBuf<uint32_t> cell(c, n), cell_counts(c, static_cast<uint64_t>(chunks) * PIV), perm(c, n);
-  pivot_assign_kernel<<<ceil_div(n, PA_PTS), 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), cell.get());
+  DevBuf<uint32_t> piv_rows(c, PIV), cell(c, n), cell_counts(c, static_cast<uint64_t>(chunks) * PIV), perm(c, n);
+  select_pivots(c, d_x, n, d, piv_rows.get());
+  DevBuf<float> score, pnorm;
+  if (prune) {
+    score.alloc(c, n * PIV);
+    pnorm.alloc(c, PIV);
+  }
+  pivot_assign_kernel<<<ceil_div(n, PA_PTS), 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), piv_rows.get(), cell.get(),
+                                                                 score.get(), pnorm.get());
   PM_LAUNCHED();
   cell_chunk_count_kernel<<<chunks, 256, 0, c.stream>>>(cell.get(), n, cell_counts.get());
   PM_LAUNCHED();
@@ -924,14 +958,13 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   cell_place_kernel<<<chunks, 32, 0, c.stream>>>(cell.get(), n, cell_counts.get(), perm.get());
   PM_LAUNCHED();
 
-  // Approximate kNN: every row block visits only the column tiles of the nprobe cells whose pivots are
-  // nearest its own cells' (own cells first), instead of every tile. The cells are contiguous ranges of
-  // the locality order: cell p starts at the first chunk's offset for p.
-  DevBuf<uint32_t> tile_ptr, tile_list;
-  if (nprobe > 0 && nprobe < PIV) {
+  // Tile lists over the cells nearest each row block: every row block visits only the column tiles of
+  // the `probe` pivot cells whose pivots are nearest its own cells' (own cells first). The cells are
+  // contiguous ranges of the locality order: cell p starts at the first chunk's offset for p.
+  auto probe_lists = [&](int probe, DevBuf<uint32_t>& tile_ptr, DevBuf<uint32_t>& tile_list) {
     std::vector<uint32_t> cstart(PIV + 1);
     DevBuf<float> piv(c, static_cast<uint64_t>(PIV) * d);
-    gather_pivots_kernel<<<PIV, 128, 0, c.stream>>>(d_x, n, static_cast<int>(d), piv.get());
+    gather_pivots_kernel<<<PIV, 128, 0, c.stream>>>(d_x, piv_rows.get(), static_cast<int>(d), piv.get());
     PM_LAUNCHED();
     std::vector<float> hp(static_cast<size_t>(PIV) * d);
     PM_CUDA(cudaMemcpyAsync(cstart.data(), cell_counts.get(), PIV * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
@@ -939,7 +972,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     PM_CUDA(cudaStreamSynchronize(c.stream));
     cstart[PIV] = static_cast<uint32_t>(n);
     // nearest pivots of each pivot (itself first), by f64 squared distance, ties to the lower index
-    std::vector<std::vector<int>> probe(PIV);
+    std::vector<std::vector<int>> near(PIV);
     std::vector<std::pair<double, int>> dd(PIV);
     for (int p = 0; p < PIV; ++p) {
       for (int q = 0; q < PIV; ++q) {
@@ -950,13 +983,12 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
         }
         dd[q] = {q == p ? -1.0 : acc, q};
       }
-      std::partial_sort(dd.begin(), dd.begin() + nprobe, dd.end());
-      for (int r = 0; r < nprobe; ++r) probe[p].push_back(dd[r].second);
+      std::partial_sort(dd.begin(), dd.begin() + probe, dd.end());
+      for (int r = 0; r < probe; ++r) near[p].push_back(dd[r].second);
     }
-    const uint64_t nblocks = n_pad / TC_BM, ntl = n_pad / TC_BN;
     std::vector<uint32_t> ptr(nblocks + 1, 0), list;
     std::vector<uint64_t> stamp(ntl, ~0ull);
-    list.reserve(nblocks * static_cast<uint64_t>(nprobe) * 40);
+    list.reserve(nblocks * static_cast<uint64_t>(probe) * 40);
     auto add_cell = [&](int q, uint64_t b) {
       if (cstart[q + 1] <= cstart[q]) return;
       for (uint64_t t = cstart[q] / TC_BN; t <= (cstart[q + 1] - 1) / TC_BN; ++t)
@@ -971,14 +1003,18 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
       for (int p = 0; p < PIV && r0 < r1; ++p)
         if (cstart[p] < r1 && cstart[p + 1] > r0) own.push_back(p);
       for (int p : own) add_cell(p, b);
-      for (int r = 1; r < nprobe; ++r)
-        for (int p : own) add_cell(probe[p][r], b);
+      for (int r = 1; r < probe; ++r)
+        for (int p : own) add_cell(near[p][r], b);
       ptr[b + 1] = static_cast<uint32_t>(list.size());
     }
     if (list.empty()) list.push_back(0);
     upload(c, tile_ptr, ptr.data(), ptr.size());
     upload(c, tile_list, list.data(), list.size());
-  }
+    return ptr;
+  };
+
+  DevBuf<uint32_t> tile_ptr, tile_list;
+  if (nprobe > 0 && nprobe < PIV) probe_lists(nprobe, tile_ptr, tile_list);
 
   DevBuf<uint16_t> H(c, n_pad * KP);
   DevBuf<float> xperm(c, n * d);
@@ -994,13 +1030,13 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     split_rows_kernel<false><<<sgrid, 256, 0, c.stream>>>(d_x, perm.get(), n, static_cast<int>(d), KP, n_pad, s, H.get(),
                                                         nrm.get(), A.get(), B.get(), partial.get(), xperm.get());
   PM_LAUNCHED();
-  std::vector<double> hp(2 * sgrid);
-  PM_CUDA(cudaMemcpyAsync(hp.data(), partial.get(), hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  std::vector<double> hpart(2 * sgrid);
+  PM_CUDA(cudaMemcpyAsync(hpart.data(), partial.get(), hpart.size() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   PM_CUDA(cudaStreamSynchronize(c.stream));
   double sa = 0.0, sb = 0.0;
   for (unsigned b = 0; b < sgrid; ++b) {
-    sa += hp[2 * b];
-    sb += hp[2 * b + 1];
+    sa += hpart[2 * b];
+    sb += hpart[2 * b + 1];
   }
   const float rho = (sa > 0.0 && sb > 0.0) ? static_cast<float>(std::sqrt(sb / sa)) : 1e-4f;
   bound_kernel<<<ceil_div(n_pad, 256), 256, 0, c.stream>>>(n, n_pad, static_cast<int>(d), KP, rho, nrm.get(), A.get(),
@@ -1032,14 +1068,10 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   DevBuf<uint2> cand(c, n_pad * C);
   DevBuf<int> ccnt(c, n_pad);
   DevBuf<uint32_t> ovf(c, n + 1), fbk(c, n + 1);
-  PM_CUDA(cudaMemsetAsync(ccnt.get(), 0xFF, n_pad * sizeof(int), c.stream));
-  PM_CUDA(cudaMemsetAsync(ovf.get() + n, 0, sizeof(uint32_t), c.stream));
-  PM_CUDA(cudaMemsetAsync(fbk.get() + n, 0, sizeof(uint32_t), c.stream));
 
   const uint32_t idesc = idesc_f16(bf16);
   // this shard's row blocks (in the locality order); the compaction and the re-rank skip the other rows
-  const uint64_t blocks = n_pad / TC_BM;
-  const uint64_t blk0 = blocks * shard.index / shard.count, blk1 = blocks * (shard.index + 1) / shard.count;
+  const uint64_t blk0 = nblocks * shard.index / shard.count, blk1 = nblocks * (shard.index + 1) / shard.count;
   const unsigned grid = static_cast<unsigned>(blk1 - blk0);
   if (shard.d_owned && blk1 > blk0) {
     const uint64_t r0 = std::min<uint64_t>(blk0 * TC_BM, n), r1 = std::min<uint64_t>(blk1 * TC_BM, n);
@@ -1048,54 +1080,93 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
       PM_LAUNCHED();
     }
   }
-  cudaEvent_t ev[2];
-  PM_CUDA(cudaEventCreate(&ev[0]));
-  PM_CUDA(cudaEventCreate(&ev[1]));
-  PM_CUDA(cudaEventRecord(ev[0], c.stream));
-  auto launch = [&](auto kern, size_t smem) {
-    PM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    if (grid == 0) return;
-    kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, KB, idesc, ge.get(), nrm.get(), perm.get(), rank,
-                                               cand.get(), ccnt.get(), ovf.get(), ovf.get() + n, c.d_err,
-                                               static_cast<int>(blk0), tile_ptr.get(), tile_list.get());
+  // One filter launch over this shard's row blocks: with tile lists (ptr, list) or over every tile.
+  auto run_filter = [&](const uint32_t* lptr, const uint32_t* llist, uint32_t* ovf_rows, uint32_t* n_ovf) {
+    PM_CUDA(cudaMemsetAsync(ccnt.get(), 0xFF, n_pad * sizeof(int), c.stream));
+    auto launch = [&](auto kern, size_t smem) {
+      PM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+      if (grid == 0) return;
+      kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, KB, idesc, ge.get(), nrm.get(), perm.get(), rank,
+                                                 cand.get(), ccnt.get(), ovf_rows, n_ovf, c.d_err,
+                                                 static_cast<int>(blk0), lptr, llist);
+    };
+    const bool p16 = PER == 16;
+    if (mode == MODE_STREAM) {
+      constexpr size_t sm = FilterLayout<0, MODE_STREAM>::SMEM;
+      if (p16) launch(knn_filter_kernel<0, 16, MODE_STREAM>, sm);
+      else launch(knn_filter_kernel<0, 32, MODE_STREAM>, sm);
+    } else if (KB == 1) {
+      constexpr size_t sm = FilterLayout<1, MODE_TILE>::SMEM;
+      if (p16) launch(knn_filter_kernel<1, 16, MODE_TILE>, sm);
+      else launch(knn_filter_kernel<1, 32, MODE_TILE>, sm);
+    } else if (KB == 2) {
+      constexpr size_t sm = FilterLayout<2, MODE_TILE>::SMEM;
+      if (p16) launch(knn_filter_kernel<2, 16, MODE_TILE>, sm);
+      else launch(knn_filter_kernel<2, 32, MODE_TILE>, sm);
+    } else if (KB == 3) {
+      constexpr size_t sm = FilterLayout<3, MODE_KBLOCK>::SMEM;
+      if (p16) launch(knn_filter_kernel<3, 16, MODE_KBLOCK>, sm);
+      else launch(knn_filter_kernel<3, 32, MODE_KBLOCK>, sm);
+    } else {
+      constexpr size_t sm = FilterLayout<4, MODE_KBLOCK>::SMEM;
+      if (p16) launch(knn_filter_kernel<4, 16, MODE_KBLOCK>, sm);
+      else launch(knn_filter_kernel<4, 32, MODE_KBLOCK>, sm);
+    }
+    PM_LAUNCHED();
   };
-  const bool p16 = PER == 16;
-  if (mode == MODE_STREAM) {
-    constexpr size_t sm = FilterLayout<0, MODE_STREAM>::SMEM;
-    if (p16) launch(knn_filter_kernel<0, 16, MODE_STREAM>, sm);
-    else launch(knn_filter_kernel<0, 32, MODE_STREAM>, sm);
-  } else if (KB == 1) {
-    constexpr size_t sm = FilterLayout<1, MODE_TILE>::SMEM;
-    if (p16) launch(knn_filter_kernel<1, 16, MODE_TILE>, sm);
-    else launch(knn_filter_kernel<1, 32, MODE_TILE>, sm);
-  } else if (KB == 2) {
-    constexpr size_t sm = FilterLayout<2, MODE_TILE>::SMEM;
-    if (p16) launch(knn_filter_kernel<2, 16, MODE_TILE>, sm);
-    else launch(knn_filter_kernel<2, 32, MODE_TILE>, sm);
-  } else if (KB == 3) {
-    constexpr size_t sm = FilterLayout<3, MODE_KBLOCK>::SMEM;
-    if (p16) launch(knn_filter_kernel<3, 16, MODE_KBLOCK>, sm);
-    else launch(knn_filter_kernel<3, 32, MODE_KBLOCK>, sm);
-  } else {
-    constexpr size_t sm = FilterLayout<4, MODE_KBLOCK>::SMEM;
-    if (p16) launch(knn_filter_kernel<4, 16, MODE_KBLOCK>, sm);
-    else launch(knn_filter_kernel<4, 32, MODE_KBLOCK>, sm);
-  }
-  PM_LAUNCHED();
-  PM_CUDA(cudaEventRecord(ev[1], c.stream));
-  c.check_errors("tensor-core kNN filter");
-  float fms = 0.0f;
-  PM_CUDA(cudaEventElapsedTime(&fms, ev[0], ev[1]));
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
-  last_tc_filter_ms() = fms;
-
   const unsigned cgrid = std::min<unsigned>(ceil_div(n, RC_WARPS), c.sm_count * 16);
-  if (PER == 16)
-    knn_compact_kernel<16><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get());
-  else
-    knn_compact_kernel<32><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get());
-  PM_LAUNCHED();
+  auto compact = [&](float* ub) {
+    if (PER == 16)
+      knn_compact_kernel<16><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get(), ub);
+    else
+      knn_compact_kernel<32><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get(), ub);
+    PM_LAUNCHED();
+  };
+  cudaEvent_t ev[3];
+  for (auto& e : ev) PM_CUDA(cudaEventCreate(&e));
+  PM_CUDA(cudaEventRecord(ev[0], c.stream));
+  st.tiles_full = static_cast<uint64_t>(grid) * ntl;
+  st.tiles_visited = st.tiles_full;
+  if (prune) {
+    // First pass: each block over the cells nearest its own gives every row a bound of its k'-th
+    // neighbour distance; then the tiles that may hold a neighbour of some row of the block.
+    DevBuf<uint32_t> aptr, alist, aovf(c, n + 1);
+    const std::vector<uint32_t> hptr = probe_lists(PRUNE_PROBE, aptr, alist);
+    st.tiles_bound = hptr[blk1] - hptr[blk0];
+    PM_CUDA(cudaMemsetAsync(aovf.get() + n, 0, sizeof(uint32_t), c.stream));
+    run_filter(aptr.get(), alist.get(), aovf.get(), aovf.get() + n);
+    c.check_errors("tensor-core kNN bound pass");
+    DevBuf<float> ub(c, n_pad);
+    compact(ub.get());
+    PruneInputs in;
+    in.perm = perm.get();
+    in.cell = cell.get();
+    in.score = score.get();
+    in.pnorm = pnorm.get();
+    in.rownorm = nrm.get();
+    in.ub = ub.get();
+    in.n = n;
+    in.n_pad = n_pad;
+    in.d = d;
+    in.inv_s = 1.0f / s;
+    in.blk0 = blk0;
+    in.blk1 = blk1;
+    st.tiles_visited = build_pruned_tile_lists(c, in, tile_ptr, tile_list);
+  }
+  PM_CUDA(cudaEventRecord(ev[1], c.stream));
+  PM_CUDA(cudaMemsetAsync(ovf.get() + n, 0, sizeof(uint32_t), c.stream));
+  PM_CUDA(cudaMemsetAsync(fbk.get() + n, 0, sizeof(uint32_t), c.stream));
+  run_filter(tile_ptr.get(), tile_list.get(), ovf.get(), ovf.get() + n);
+  PM_CUDA(cudaEventRecord(ev[2], c.stream));
+  c.check_errors("tensor-core kNN filter");
+  float fms = 0.0f, bms = 0.0f;
+  PM_CUDA(cudaEventElapsedTime(&bms, ev[0], ev[1]));
+  PM_CUDA(cudaEventElapsedTime(&fms, ev[1], ev[2]));
+  for (auto& e : ev) cudaEventDestroy(e);
+  st.filter_ms = fms;
+  st.bound_ms = bms;
+
+  compact(nullptr);
   const int di = static_cast<int>(d), ki = static_cast<int>(kp);
   auto rerank = [&](auto kern, int warps) {
     const unsigned rgrid = std::min<unsigned>(ceil_div(n, warps), c.sm_count * 32);
@@ -1120,7 +1191,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_CUDA(cudaMemcpyAsync(&counts[0], ovf.get() + n, 4, cudaMemcpyDeviceToHost, c.stream));
   PM_CUDA(cudaMemcpyAsync(&counts[1], fbk.get() + n, 4, cudaMemcpyDeviceToHost, c.stream));
   PM_CUDA(cudaStreamSynchronize(c.stream));
-  last_tc_fallback_rows() = counts[0] + counts[1];
+  st.fallback_rows = counts[0] + counts[1];
   const uint32_t* lists[2] = {ovf.get(), fbk.get()};
   for (int q = 0; q < 2; ++q) {
     if (!counts[q]) continue;
@@ -1129,13 +1200,8 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   return true;
 }
 
-double& last_tc_filter_ms() {
-  static thread_local double v = 0.0;
-  return v;
-}
-
-uint64_t& last_tc_fallback_rows() {
-  static thread_local uint64_t v = 0;
+KnnTcStats& last_tc_stats() {
+  static thread_local KnnTcStats v;
   return v;
 }
 

@@ -124,13 +124,16 @@ class PairConfiguration:
 
 
 class KnnMode:
-    """How the exact kNN is computed (engine switch; every mode returns the same indices)."""
+    """How the kNN is computed (engine switch). Modes 0-3 and 5 return identical exact indices and
+    distances; mode 4 (APPROX) is approximate from ``approx_threshold`` rows on. From 32,768 rows the
+    tensor-core modes 0-2 skip column tiles that provably hold no neighbour; mode 5 computes every tile."""
 
     AUTO = 0
     TENSOR_F16 = 1
     TENSOR_BF16 = 2
     SIMT_EXACT = 3
     APPROX = 4  # approximate at n >= approx_threshold (16 of 256 pivot cells per row block); exact below
+    TENSOR_F16_FULL = 5  # TENSOR_F16 without tile pruning
 
 
 class Metric:
@@ -294,7 +297,7 @@ def quality(x, y, sample, triplets, k: int = 10, device: int = 0):
 
 
 STAGES = ("preprocess", "knn", "reselect", "sample_mn", "sample_fp", "csr", "init", "optimize", "knn_filter",
-          "knn_fallback_rows")
+          "knn_fallback_rows", "knn_bound", "knn_tiles_visited", "knn_tiles_full", "knn_tiles_bound")
 
 
 def set_stage_timing(enabled: bool) -> None:

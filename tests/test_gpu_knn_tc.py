@@ -118,6 +118,59 @@ def test_tc_knn_full_1m_x_128(lib, orc):
     assert (gi < x.shape[0]).all() and not (gi == np.arange(x.shape[0], dtype=np.uint32)[:, None]).any()
 
 
+F16_FULL = 5
+
+
+def _pruned_stats(lib, x, k):
+    """One fit_transform of one iteration with stage timing on: the kNN stage's tile counters."""
+    lib.set_stage_timing(True)
+    try:
+        lib.fit_transform(x, lib.Configuration(seed=3, initialization=lib.Initialization.Random(1),
+                                               override_neighbors=k, num_iters=(0, 0, 1)))
+        return lib.stage_times()
+    finally:
+        lib.set_stage_timing(False)
+
+
+@pytest.mark.parametrize("gen,n,d,k", [("aniso", 60000, 128, 90), ("subspace", 50000, 256, 99),
+                                       ("iso", 40000, 64, 60), ("uniform", 40000, 32, 30),
+                                       ("dups", 40000, 24, 60)])
+def test_tile_pruning_equals_full_sweep(lib, orc, gen, n, d, k):
+    """From 32,768 rows the tensor-core kNN skips column tiles that provably hold no neighbour; the result
+    must equal the full sweep (mode 5) bit for bit, and the oracle on sampled rows, on clustered data
+    (much pruned), uniform data (little pruned) and exact duplicates (overflow rows)."""
+    from pacmap_b200 import datasets
+
+    if gen == "aniso":
+        x, _ = datasets.anisotropic_mixture(n=n, d=d, k=50, seed=4)
+    elif gen == "subspace":
+        x, _ = datasets.subspace_mixture(n=n, d=d, k=200, seed=4)
+    elif gen == "iso":
+        x = _mix(n, d, seed=4)
+    elif gen == "uniform":
+        x = np.random.default_rng(4).random((n, d), dtype=np.float32)
+    else:
+        x = _mix(n, d, seed=5)
+        x[1000:1700] = x[5]
+    xp = lib.stages.preprocess(x)[0]
+    fi, fd = lib.knn.find_k_nearest_neighbors(xp, k, knn_mode=F16_FULL)
+    gi, gd = _sampled_rows_vs_oracle(lib, orc, xp, k, 300, seed=2, knn_mode=AUTO)
+    assert np.array_equal(gd, fd)
+    assert np.array_equal(gi, fi)
+
+
+def test_tile_pruning_skips_most_tiles_on_clustered_data(lib):
+    # 100,000 x 128 of the 1M x 128 generator (50 clusters): most (row block, tile) pairs are skipped
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.anisotropic_mixture(n=100000, d=128, k=50, seed=0, draw_seed=6)
+    st = _pruned_stats(lib, x, 40)
+    frac = st["knn_tiles_visited"] / st["knn_tiles_full"]
+    print(f"tiles visited {st['knn_tiles_visited']:.0f} of {st['knn_tiles_full']:.0f} ({frac:.3f}); bound pass "
+          f"{st['knn_tiles_bound']:.0f}; filter {st['knn_filter']:.2f} ms, bound {st['knn_bound']:.2f} ms")
+    assert 0 < frac < 0.25
+
+
 def test_simt_knn_key_slices(lib, orc):
     # 9,000 rows on the exact SIMT path: the keys are split into two slices whose lists are merged
     x = _mix(9000, 16, seed=4)
