@@ -82,6 +82,8 @@ def lib():
         "orc_init_random": (None, [_u64, _u64, _u64, _f32p]),
         "orc_optimize": (C.c_int, [_f32p, _u64, _u64, _u32p, _u64, _u32p, _u64, _u32p, _u64, C.c_float,
                                    _u64, _u64, _u64, _vp, _u64, _vp, _vp]),
+        "orc_optimize_parallel": (C.c_int, [_f32p, _u64, _u64, _u32p, _u64, _u32p, _u64, _u32p, _u64, C.c_float,
+                                            _u64, _u64, _u64]),
         "orc_step": (C.c_int, [_f32p, _f32p, _f32p, _u64, _u64, _u32p, _u64, _u32p, _u64, _u32p, _u64,
                                C.c_float, _u64, _u64, _u64, _vp, _vp, _vp]),
         "orc_generate_pairs": (C.c_int, [_f32p, _u64, _u64, _u64, _u64, _u64, _u64, _u32p, _u32p, _u32p]),
@@ -271,6 +273,17 @@ def optimize(y0, pnn, pmn, pfp, lr=1.0, num_iters=(100, 100, 250), snapshots=Non
     _check(lib().orc_optimize(y, n, dim, pnn, len(pnn), pmn, len(pmn), pfp, len(pfp), lr, *num_iters,
                               _ptr(snaps), 0 if snaps is None else len(snaps), _ptr(sout), _ptr(loss)), "optimize")
     return y, sout, loss
+
+
+def optimize_parallel(y0, pnn, pmn, pfp, lr=1.0, num_iters=(100, 100, 250)):
+    """The reference's parallel optimiser loop (gradient.rs:35-151 chunked private arrays + adam.rs) for the
+    timed CPU baseline; its sums are ordered by thread, not pinned (use ``optimize`` for parity)."""
+    y = np.array(y0, dtype=np.float32, copy=True, order="C")
+    n, dim = y.shape
+    pnn, pmn, pfp = _u32(pnn).reshape(-1, 2), _u32(pmn).reshape(-1, 2), _u32(pfp).reshape(-1, 2)
+    _check(lib().orc_optimize_parallel(y, n, dim, pnn, len(pnn), pmn, len(pmn), pfp, len(pfp), lr, *num_iters),
+           "optimize_parallel")
+    return y
 
 
 def step(y, m, v, pnn, pmn, pfp, lr, p1, p2, itr, with_grad=True):

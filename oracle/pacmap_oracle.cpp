@@ -691,6 +691,112 @@ int orc_optimize(float* y, uint64_t n, uint64_t dim, const uint32_t* pnn, uint64
 
 // One optimiser step from a given (y, m, v) state at iteration `itr`: the per-iteration parity
 // harness. grad_out (optional) receives the (n+1) x dim gradient of that step.
+// The reference's parallel optimiser loop, for the timed CPU baseline (the parity paths above stay
+// sequential so that their sums have one fixed order). gradient.rs:35-74: the three pair lists cut into
+// chunks of 128 * 1024 pairs; every chunk computes its contributions into its own zeroed (n+1) x dim
+// array (process_pairs, gradient.rs:98-151) and the chunk arrays are folded and reduced across the
+// worker threads (rayon par_bridge + reduce; here OpenMP threads fold in chunk order, then the thread
+// accumulators are summed in thread order). adam.rs:35-60 with the element loop split across threads
+// (Zip::par_for_each). The sums' order differs from the sequential oracle (as rayon's does between runs).
+int orc_optimize_parallel(float* y, uint64_t n, uint64_t dim, const uint32_t* pnn, uint64_t n_nn, const uint32_t* pmn,
+                          uint64_t n_mnp, const uint32_t* pfp, uint64_t n_fpp, float lr, uint64_t p1, uint64_t p2,
+                          uint64_t p3) {
+  const uint64_t cnt = n * dim, gsz = (n + 1) * dim;
+  constexpr uint64_t CHUNK = 128 * 1024;
+  struct L { const uint32_t* p; uint64_t cnt; float dc, wc; bool fp; };
+  const L lists[3] = {{pnn, n_nn, 10.0f, 20.0f, false}, {pmn, n_mnp, 10000.0f, 20000.0f, false},
+                      {pfp, n_fpp, 1.0f, 2.0f, true}};
+  std::vector<std::pair<int, uint64_t>> chunks;  // (list, first pair)
+  for (int l = 0; l < 3; ++l)
+    for (uint64_t a = 0; a < lists[l].cnt; a += CHUNK) chunks.push_back({l, a});
+  for (int l = 0; l < 3; ++l)
+    for (uint64_t q = 0; q < 2 * lists[l].cnt; ++q)
+      if (lists[l].p[q] >= n) return ORC_ERR_PAIR_INDEX;
+  std::vector<float> m(cnt, 0.0f), v(cnt, 0.0f), grad(gsz);
+#ifdef _OPENMP
+  const int nt = omp_get_max_threads();
+#else
+  const int nt = 1;
+#endif
+  std::vector<std::vector<float>> acc(nt, std::vector<float>(gsz));
+  std::vector<float> tloss(nt);
+  const uint64_t total = p1 + p2 + p3;
+  for (uint64_t itr = 0; itr < total; ++itr) {
+    float w3[3];
+    orc_weights(itr, p1, p2, 1000.0f, w3);
+    const float wl[3] = {w3[1], w3[0], w3[2]};
+#pragma omp parallel
+    {
+#ifdef _OPENMP
+      const int t = omp_get_thread_num();
+#else
+      const int t = 0;
+#endif
+      std::vector<float>& a = acc[t];
+      std::fill(a.begin(), a.end(), 0.0f);
+      float lsum = 0.0f;
+      std::vector<float> g(gsz), yij(dim);
+#pragma omp for schedule(dynamic, 1)
+      for (int64_t ci = 0; ci < static_cast<int64_t>(chunks.size()); ++ci) {
+        const L& l = lists[chunks[ci].first];
+        const float w = wl[chunks[ci].first];
+        const uint64_t b0 = chunks[ci].second, b1 = std::min<uint64_t>(b0 + CHUNK, l.cnt);
+        std::fill(g.begin(), g.end(), 0.0f);  // process_pairs: Array2::zeros((n + 1, dim))
+        float loss = 0.0f;
+        for (uint64_t p = b0; p < b1; ++p) {
+          const uint64_t i = l.p[2 * p], j = l.p[2 * p + 1];
+          if (i == j) continue;
+          float dij = 1.0f;
+          for (uint64_t c = 0; c < dim; ++c) {
+            yij[c] = y[i * dim + c] - y[j * dim + c];
+            dij = dij + yij[c] * yij[c];
+          }
+          float w1;
+          if (l.fp) {
+            loss = loss + w * (1.0f / (1.0f + dij));
+            const float tt = 1.0f + dij;
+            w1 = w * (2.0f / (tt * tt));
+          } else {
+            loss = loss + w * (dij / (l.dc + dij));
+            const float tt = l.dc + dij;
+            w1 = w * (l.wc / (tt * tt));
+          }
+          for (uint64_t c = 0; c < dim; ++c) {
+            const float gu = w1 * yij[c];
+            if (l.fp) {
+              g[i * dim + c] -= gu;
+              g[j * dim + c] += gu;
+            } else {
+              g[i * dim + c] += gu;
+              g[j * dim + c] -= gu;
+            }
+          }
+        }
+        for (uint64_t e = 0; e < gsz; ++e) a[e] += g[e];  // reduce: grad1 += &grad2
+        lsum += loss;
+      }
+      tloss[t] = lsum;
+    }
+    std::fill(grad.begin(), grad.end(), 0.0f);
+    float loss = 0.0f;
+    for (int t = 0; t < nt; ++t) {
+      for (uint64_t e = 0; e < gsz; ++e) grad[e] += acc[t][e];
+      loss += tloss[t];
+    }
+    grad[n * dim] = loss;
+    const int it = static_cast<int>(itr + 1);
+    const float lr_t = lr * std::sqrt(1.0f - powi_f32(0.999f, it)) / (1.0f - powi_f32(0.9f, it));
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < static_cast<int64_t>(cnt); ++e) {
+      const float gg = grad[e];
+      m[e] = m[e] + (1.0f - 0.9f) * (gg - m[e]);
+      v[e] = v[e] + (1.0f - 0.999f) * (gg * gg - v[e]);
+      y[e] = y[e] - lr_t * m[e] / (std::sqrt(v[e]) + 1e-7f);
+    }
+  }
+  return ORC_OK;
+}
+
 int orc_step(float* y, float* m, float* v, uint64_t n, uint64_t dim, const uint32_t* pnn, uint64_t n_nn,
              const uint32_t* pmn, uint64_t n_mnp, const uint32_t* pfp, uint64_t n_fpp, float lr, uint64_t p1,
              uint64_t p2, uint64_t itr, float* grad_out, double* grad64_out, float* abs_sum_out) {
