@@ -283,8 +283,10 @@ pacmap_status pacmap_quality(const float* x, uint64_t n, uint64_t d, const float
  * d_x, d_out: n x d device buffers on `device`; `stream` is a cudaStream_t (NULL = legacy default
  * stream). Stream-ordered: the call returns once the work is enqueued. The scratch is a fixed device
  * array of the library (at most 16,384 columns; larger d returns PACMAP_ERR_UNSUPPORTED), looked up on
- * the first call per device -- make that call before any stream capture. All calls share that array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * the first call per device -- make that call before any stream capture -- and again on every call whose
+ * stream is not capturing (the address belongs to the device's primary context). The caller's current
+ * device is restored before the call returns. All calls share that array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 pacmap_status pacmap_preprocess_noalloc(const float* d_x, uint64_t n, uint64_t d, float* d_out, void* stream,
                                         int32_t device);
 

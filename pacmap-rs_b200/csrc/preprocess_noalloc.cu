@@ -6,10 +6,13 @@
 // below, which every GPU that loads the library holds until the process exits.
 //
 // The first call on a device looks up that array's device address (cudaGetSymbolAddress, with the
-// device current) and caches it; make that first call before any stream capture. Every call shares the
-// one array and leaves its contents behind: the min/max keys are reset at the start of each call, the
-// means are overwritten. Calls that overlap on the GPU (two streams, or two host threads) race on the
-// array and must be serialised by the caller.
+// device current) and caches it; make that first call before any stream capture. The address belongs to
+// the device's primary context, so every call whose stream is not capturing looks it up again (after a
+// cudaDeviceReset the cached one would be stale); a capturing call uses the cached one. The caller's
+// current device is restored before the call returns. Every call shares the one array and leaves its
+// contents behind: the min/max keys are reset at the start of each call, the means are overwritten.
+// Calls that overlap on the GPU (two streams, or two host threads) race on the array and must be
+// serialised by the caller.
 #include <mutex>
 
 #include "engine.cuh"
@@ -95,10 +98,11 @@ __global__ void na_normalize_kernel(const float* __restrict__ x, uint64_t n, uin
   }
 }
 
-// The scratch array's device address on `device` (looked up once per device, that device current).
-uint32_t* scratch_address(int device) {
+// The scratch array's device address on `device` (that device current): looked up on a device's first
+// call and on every call whose stream is not capturing (`refresh`), cached for capturing calls.
+uint32_t* scratch_address(int device, bool refresh) {
   std::lock_guard<std::mutex> g(g_noalloc_mutex);
-  if (g_noalloc_addr[device]) return g_noalloc_addr[device];
+  if (g_noalloc_addr[device] && !refresh) return g_noalloc_addr[device];
   void* p = nullptr;
   const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (e != cudaSuccess || p == nullptr)
@@ -112,8 +116,25 @@ uint32_t* scratch_address(int device) {
 
 using namespace pacmap;
 
+namespace {
+// Puts the caller's current device back when the call returns, on every path.
+struct RestoreDevice {
+  int prev = -1;
+  RestoreDevice() {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+  }
+  ~RestoreDevice() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+}  // namespace
+
 extern "C" pacmap_status pacmap_preprocess_noalloc(const float* d_x, uint64_t n, uint64_t d, float* d_out,
                                                    void* stream, int32_t device) {
+  RestoreDevice restore;
   try {
     PM_REQUIRE(d_x != nullptr && d_out != nullptr, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
     PM_REQUIRE(n * d > 0, PACMAP_ERR_EMPTY_ARRAY_MIN_MAX, "Failed to compute min or max of X: the array is empty");
@@ -131,7 +152,9 @@ extern "C" pacmap_status pacmap_preprocess_noalloc(const float* d_x, uint64_t n,
     PM_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
     PM_REQUIRE(major == 10, PACMAP_ERR_NO_DEVICE, "device is not compute capability 10.x (sm_100)");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    uint32_t* keys = scratch_address(device);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PM_CUDA(cudaStreamIsCapturing(s, &cap));
+    uint32_t* keys = scratch_address(device, cap == cudaStreamCaptureStatusNone);
     float* mean = reinterpret_cast<float*>(keys + 4);
     na_reset_keys_kernel<<<1, 32, 0, s>>>(keys);
     PM_LAUNCHED();

@@ -41,6 +41,33 @@ def test_noalloc_preprocess_matches_allocating_entry_point(lib):
         assert np.array_equal(got, expected)
 
 
+def test_noalloc_in_place_small_n_keeps_device_and_memory(lib):
+    import torch
+
+    fn = _entry(lib)
+    stream = torch.cuda.current_stream()
+    # n < 512 (one column-sum chunk), and the output written over the input
+    x = np.random.default_rng(13).uniform(-1.0, 4.0, size=(300, 65)).astype(np.float32)
+    expected, *_ = lib.stages.preprocess(x)
+    dx = torch.from_numpy(x).cuda()
+    rc = fn(C.c_void_p(dx.data_ptr()), 300, 65, C.c_void_p(dx.data_ptr()), C.c_void_p(stream.cuda_stream), 0)
+    stream.synchronize()
+    assert rc == 0, lib._abi.last_error()
+    assert np.array_equal(dx.cpu().numpy(), expected)
+    # later calls take no device memory: free memory is unchanged across two more calls
+    y = torch.from_numpy(np.random.default_rng(14).normal(size=(2000, 48)).astype(np.float32)).cuda()
+    out = torch.empty_like(y)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        assert fn(C.c_void_p(y.data_ptr()), 2000, 48, C.c_void_p(out.data_ptr()), None, 0) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    # the caller's current device is left as it was
+    assert torch.cuda.current_device() == 0
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch(lib):
     import torch
 
