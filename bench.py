@@ -242,11 +242,12 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def _pair_counts(n, mid_near_ratio=0.5, far_pair_ratio=2.0):
-    """decide_num_pairs (lib.rs:565-597) in f32: (k, n_mn, n_fp)."""
-    rnd = lambda v: int(np.floor(np.float32(v) + np.float32(0.5)))  # noqa: E731  (f32::round: half away from 0)
-    k = 10 if n <= 10000 else rnd(np.float32(10.0) + np.float32(15.0) * (np.log10(np.float32(n)) - np.float32(4.0)))
-    return k, rnd(np.float32(k) * np.float32(mid_near_ratio)), rnd(np.float32(k) * np.float32(far_pair_ratio))
+def _pair_counts(n):
+    """decide_num_pairs (lib.rs:565-597) as the library computes it: (k, n_mn, n_fp) read back through its
+    C ABI (no device needed), default ratios."""
+    import pacmap_b200 as pm
+
+    return pm.decide_num_pairs(n)
 
 
 def _optimize_bytes(n, dim, iters):

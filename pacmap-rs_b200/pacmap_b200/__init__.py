@@ -284,6 +284,17 @@ def fit_transform_device(x_ptr: int, n: int, d: int, out_ptr: int, config: Optio
                                                   C.c_void_p(snapshots_ptr) if snapshots_ptr else None))
 
 
+def decide_num_pairs(n: int, config: Optional[Configuration] = None):
+    """(k, n_mn, n_fp) of ``decide_num_pairs`` (lib.rs:565-597) as the library computes it for n points
+    (k clamped to n - 1), through ``pacmap_generate_pairs`` with no output buffers: no device is needed."""
+    cfg = config if config is not None else Configuration()
+    cc = _CConfig(cfg, n)
+    counts = np.zeros(3, np.uint64)
+    dummy = np.zeros(1, np.float32)  # not read when only the counts are asked for
+    _check(_abi.lib().pacmap_generate_pairs(ptr(dummy), n, 1, C.byref(cc.c), ptr(counts), None, None, None))
+    return tuple(int(v) for v in counts)
+
+
 def quality(x, y, sample, triplets, k: int = 10, device: int = 0):
     """(k-NN preservation over `sample`, triplet-order accuracy over `triplets`) on the GPU."""
     x = np.ascontiguousarray(x, dtype=np.float32)

@@ -91,3 +91,18 @@ def test_no_device_is_an_error_not_a_fallback(lib):
         lib.fit_transform(x, lib.Configuration(initialization=lib.Initialization.Random(0)))
     with pytest.raises(lib.NoDevice):
         lib.knn.find_k_nearest_neighbors(x, 3)
+
+
+@pytest.mark.parametrize("n", [2, 11, 2000, 10000, 10001, 60000, 200000, 1_000_000, 4_000_000, 2**31 + 5])
+def test_library_pair_counts_equal_the_oracle_at_every_size(lib, orc, n):
+    # decide_num_pairs (lib.rs:565-597) as the library computes it in f32, read back through the C ABI
+    # (pacmap_generate_pairs with no output buffers needs no device), against the oracle's restatement
+    for cfg_kw, orc_kw in [({}, {}), ({"mid_near_ratio": 0.3, "far_pair_ratio": 1.5}, {"mn_ratio": 0.3, "fp_ratio": 1.5}),
+                           ({"override_neighbors": 7}, {"override": 7})]:
+        got = lib.decide_num_pairs(n, lib.Configuration(**cfg_kw))
+        rc, (k, n_mn, n_fp) = orc.decide_num_pairs(n, **orc_kw)
+        assert rc == 0
+        assert got == (min(k, n - 1), n_mn, n_fp), (n, cfg_kw)
+    if n in (60000, 200000, 1_000_000, 4_000_000):
+        assert lib.decide_num_pairs(n) == {60000: (22, 11, 44), 200000: (30, 15, 60), 1_000_000: (40, 20, 80),
+                                          4_000_000: (49, 25, 98)}[n]
