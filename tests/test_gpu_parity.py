@@ -132,6 +132,41 @@ def test_fp_distribution_uniform(lib, orc):
     assert chi2 < n + 6 * np.sqrt(2 * n)  # df ~ n
 
 
+def test_mn_distribution_is_the_second_of_six_rule(lib, orc):
+    """sampling.rs:118-142,296-313: each mid-near partner is the 2nd closest of 6 distinct uniform draws
+    (excluding the point and its earlier picks). The rank of the partner's distance among all n - 1 other
+    points, divided by n, then follows the 2nd order statistic of 6 uniforms, Beta(2, 5): KS test of the
+    GPU's draws against it, and two-sample KS against the rule run with numpy's own generator."""
+    from scipy import stats
+
+    n, d, n_mn = 3000, 10, 5
+    x = _mixture(n, d, seed=8)
+    xp, *_ = orc.preprocess(x)
+    pmn, _ = lib.stages.sample_pairs(xp, np.zeros((n * 10, 2), np.uint32), 10, n_mn, 0, 2024)
+    dist = np.sqrt(((xp[:, None, :] - xp[None, :, :]) ** 2).sum(-1))
+    np.fill_diagonal(dist, np.inf)
+    order = np.argsort(np.argsort(dist, axis=1, kind="stable"), axis=1, kind="stable")  # rank of j in row i
+    i, j = pmn[:, 0].astype(np.int64), pmn[:, 1].astype(np.int64)
+    u_gpu = (order[i, j] + 0.5) / (n - 1)
+    rng = np.random.default_rng(5)
+    u_ref = []
+    for r in range(n):
+        picked = []
+        for _ in range(n_mn):
+            cand = []
+            while len(cand) < 6:
+                c = int(rng.integers(n))
+                if c != r and c not in picked and c not in cand:
+                    cand.append(c)
+            c2 = sorted(cand, key=lambda c: (dist[r, c], cand.index(c)))[1]
+            picked.append(c2)
+            u_ref.append((order[r, c2] + 0.5) / (n - 1))
+    ks_beta = stats.kstest(u_gpu, "beta", args=(2, 5))
+    ks_two = stats.ks_2samp(u_gpu, np.array(u_ref))
+    print(f"MN rank KS vs Beta(2,5): p={ks_beta.pvalue:.3f}; vs the rule on numpy draws: p={ks_two.pvalue:.3f}")
+    assert ks_beta.pvalue > 1e-3 and ks_two.pvalue > 1e-3
+
+
 # ----------------------------------------------------------------------------------------------------
 # Gradient and optimiser (gradient.rs, adam.rs, weights.rs, lib.rs:800-837).
 # ----------------------------------------------------------------------------------------------------
