@@ -305,6 +305,12 @@ void* pacmap_device_stream(int32_t device);
 /* Kernel launches issued by this thread since the last call of this function (diagnostics). */
 uint64_t pacmap_take_launch_count(void);
 
+/* Failure-detection test hook (no reference analogue; tests only). With on != 0, the tensor-core kNN
+ * filter on `device` issues none of its operand copies, so its bounded wait on them runs out (2 s) and
+ * every later kNN call fails with PACMAP_ERR_DEVICE_INVARIANT ("a bounded device wait timed out") instead
+ * of hanging; on = 0 restores normal operation. The caller's current device is kept. */
+pacmap_status pacmap_debug_stall_knn_loads(int32_t device, int32_t on);
+
 /* The message of the last failure on this thread ("" after success). */
 const char* pacmap_last_error(void);
 

@@ -490,6 +490,11 @@ __global__ void bound_kernel(uint64_t n, uint64_t n_pad, int d, int KP, float rh
 // ---------------------------------------------------------------------------------------------
 // 2. the tcgen05 filter
 // ---------------------------------------------------------------------------------------------
+// Failure-detection test hook (pacmap_debug_stall_knn_loads): when non-zero, the filter's TMA producer
+// issues no load and raises nothing itself, so the MMA warp's bounded wait on the operands runs out
+// (2 s), raises DEV_ERR_TIMEOUT and aborts the block -- the path a lost copy would take. Zero otherwise.
+__device__ int g_debug_stall_loads = 0;
+
 // K blocks of 64 elements: KP = 64 * KB (KB = 0: run-time kb_rt, MODE_STREAM only); candidate buffer
 // C = 32 * PER per row.
 template <int KB, int PER, int MODE>
@@ -558,7 +563,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
   if (warp == 0) {
     // ------------------------------- TMA producer -------------------------------
     if (lane == 0) {
-      if (MODE != MODE_STREAM) {
+      const bool stall = *reinterpret_cast<volatile int*>(&g_debug_stall_loads) != 0;
+      const bool a_issued = MODE != MODE_STREAM && !stall;
+      if (a_issued) {
         mbar_expect_tx(&sh->a_full, L::A_RES);
         for (int h = 0; h < 2; ++h)
           for (int kb = 0; kb < KB; ++kb)
@@ -567,7 +574,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
       const int total = nt * nch;
       int issued = 0, s = 0, ph = 0;
       bool stop = false;
-      for (int t = 0; t < nt && !stop; ++t) {
+      for (int t = 0; t < nt && !stop && !stall; ++t) {
         const int tile = tile_at(t);
         for (int ch = 0; ch < nch; ++ch) {
           if (issued >= NST && !mbar_wait(&sh->empty[s], ph ^ 1, abort_flag)) {
@@ -594,12 +601,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
           }
         }
       }
-      if (issued < total) {
+      if (issued < total && !stall) {
         atomicOr(err, DEV_ERR_TIMEOUT);
         sh->abort_flag = 1;
       }
-      // Drain: every issued load has landed before the block may exit.
-      if (MODE != MODE_STREAM) mbar_wait(&sh->a_full, 0, abort_flag);
+      // Drain: every issued load has landed before the block may exit (bounded, whatever the abort flag).
+      if (a_issued) {
+        const uint64_t t0 = globaltimer();
+        while (!mbar_try_wait(&sh->a_full, 0) && globaltimer() - t0 < WAIT_LIMIT_NS) {
+        }
+      }
       for (int q = (issued > NST ? issued - NST : 0); q < issued; ++q) {
         const uint64_t t0 = globaltimer();
         while (!mbar_try_wait(&sh->full[q % NST], (q / NST) & 1) && globaltimer() - t0 < WAIT_LIMIT_NS) {
@@ -1206,3 +1217,31 @@ KnnTcStats& last_tc_stats() {
 }
 
 }  // namespace pacmap
+
+extern "C" pacmap_status pacmap_debug_stall_knn_loads(int32_t device, int32_t on) {
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) {
+    cudaGetLastError();
+    prev = -1;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    pacmap::set_last_error("no CUDA device is visible");
+    return PACMAP_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) {
+    pacmap::set_last_error("device ordinal " + std::to_string(device) + " is not available");
+    return PACMAP_ERR_INVALID_ARGUMENT;
+  }
+  const int v = on ? 1 : 0;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(pacmap::g_debug_stall_loads, &v, sizeof(int));
+  if (prev >= 0) cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    pacmap::set_last_error(std::string("cudaMemcpyToSymbol: ") + cudaGetErrorString(e));
+    return PACMAP_ERR_CUDA;
+  }
+  pacmap::set_last_error("");
+  return PACMAP_OK;
+}

@@ -128,6 +128,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) gemm_tn_kernel(const __grid_c
         sh->abort_flag = 1;
       }
       umma_commit(&sh->done);
+      // Every issued MMA has completed before the tensor memory is released (bounded, whatever the abort
+      // flag: the epilogue's own wait gives up at once on abort).
+      const uint64_t t0 = globaltimer();
+      while (!mbar_try_wait(&sh->done, 0) && globaltimer() - t0 < WAIT_LIMIT_NS) {
+      }
     }
   } else {
     const int quad = warp & 3;

@@ -171,6 +171,24 @@ def test_tile_pruning_skips_most_tiles_on_clustered_data(lib):
     assert 0 < frac < 0.25
 
 
+def test_bounded_wait_runs_out_with_a_status_and_the_next_call_succeeds(lib, orc):
+    """Failure detection without a GPU fault: with the test hook on, the filter's operand copies are never
+    issued, so its bounded mbarrier wait runs out; the call returns DEVICE_INVARIANT (a timeout), the block
+    releases its tensor memory, and the next call on the same context is exact again."""
+    x = _mix(3000, 64, seed=12)
+    stall = lib._abi.lib().pacmap_debug_stall_knn_loads
+    try:
+        assert stall(0, 1) == 0
+        with pytest.raises(lib.DeviceInvariant) as e:
+            lib.knn.find_k_nearest_neighbors(x, 30, knn_mode=F16)
+        assert "timed out" in str(e.value)
+    finally:
+        assert stall(0, 0) == 0
+    gi, gd = lib.knn.find_k_nearest_neighbors(x, 30, knn_mode=F16)
+    ei, ed = orc.knn_exact(x, 30)
+    assert np.array_equal(gd, ed) and np.array_equal(gi, ei)
+
+
 def test_simt_knn_key_slices(lib, orc):
     # 9,000 rows on the exact SIMT path: the keys are split into two slices whose lists are merged
     x = _mix(9000, 16, seed=4)
