@@ -158,6 +158,13 @@ pacmap_status pacmap_knn_exact_shard(const float* x, uint64_t n, uint64_t d, uin
                                      uint32_t shard, uint32_t n_shards, int32_t device, uint32_t* out_idx,
                                      float* out_dist, uint8_t* out_owned);
 
+/* pacmap_knn_exact_shard with d_x, the outputs and the owned mask in device memory of `device` (no
+ * reference analogue): the shard stays on the GPU for a collective assembly (pacmap_b200.knn). The call
+ * returns when the shard is complete. */
+pacmap_status pacmap_knn_exact_shard_device(const float* d_x, uint64_t n, uint64_t d, uint64_t k, int32_t knn_mode,
+                                            uint32_t shard, uint32_t n_shards, int32_t device, uint32_t* d_out_idx,
+                                            float* d_out_dist, uint8_t* d_out_owned);
+
 /* --- stage entry points: the parity harness and callers that run part of the pipeline --- */
 
 /* preprocess_x non-PCA branch (src/lib.rs:485-511): out = (x - min) / max - column mean. x, out: n x d.

@@ -636,6 +636,33 @@ pacmap_status pacmap_knn_exact_shard(const float* x, uint64_t n, uint64_t d, uin
   });
 }
 
+pacmap_status pacmap_knn_exact_shard_device(const float* d_x, uint64_t n, uint64_t d, uint64_t k, int32_t knn_mode,
+                                            uint32_t shard, uint32_t n_shards, int32_t device, uint32_t* d_out_idx,
+                                            float* d_out_dist, uint8_t* d_out_owned) {
+  return guarded([&] {
+    PM_REQUIRE(n_shards >= 1 && shard < n_shards, PACMAP_ERR_INVALID_ARGUMENT, "shard must be < n_shards");
+    if (n == 0) return;
+    const uint64_t kp = std::min<uint64_t>(k, n - 1);
+    PM_REQUIRE(d_x && d_out_owned && (kp == 0 || (d_out_idx && d_out_dist)), PACMAP_ERR_INVALID_ARGUMENT,
+               "NULL buffer");
+    PM_REQUIRE(knn_mode >= 0 && knn_mode <= 5, PACMAP_ERR_INVALID_ARGUMENT, "unknown knn_mode");
+    DeviceLock dl(device);
+    Ctx& c = dl.ctx;
+    PM_CUDA(cudaMemsetAsync(d_out_owned, 0, n, c.stream));
+    if (kp > 0) {
+      PM_CUDA(cudaMemsetAsync(d_out_idx, 0, n * kp * sizeof(uint32_t), c.stream));
+      PM_CUDA(cudaMemsetAsync(d_out_dist, 0, n * kp * sizeof(float), c.stream));
+      KnnShard sh;
+      sh.index = shard;
+      sh.count = n_shards;
+      sh.d_owned = d_out_owned;
+      knn_exact_device(c, d_x, n, d, kp, knn_mode, d_out_idx, d_out_dist, sh);
+    }
+    PM_CUDA(cudaStreamSynchronize(c.stream));
+    c.check_errors("knn shard");
+  });
+}
+
 pacmap_status pacmap_preprocess(const float* x, uint64_t n, uint64_t d, int32_t device, float* out, float* out_min,
                                 float* out_max, float* out_mean) {
   return guarded([&] {

@@ -221,6 +221,12 @@ def test_knn_shards_partition_rows_and_reproduce_the_full_result(lib, mode, n, d
         assert not si[~own].any() and not sd[~own].any()
     assert (cover == 1).all()
     assert np.array_equal(ui, gi) and np.array_equal(ud, gd)
+    # the device-buffer shard entry point (the NCCL assembly's input) writes the same rows
+    for s in range(3):
+        di, dd, down = lib.knn._shard_device(x, k, s, 3, mode, 0)
+        own = down.cpu().numpy()
+        assert np.array_equal(di.cpu().numpy().view(np.uint32)[own], gi[own])
+        assert np.array_equal(dd.cpu().numpy()[own], gd[own])
 
 
 APPROX = 4

@@ -44,9 +44,13 @@ def _worker(rank, world, port, q):
         import oracle
 
         x = _data()
-        idx, d = knn.find_k_nearest_neighbors_distributed(x, 15, shard_fn=_oracle_shard)
+        st = {}
+        idx, d = knn.find_k_nearest_neighbors_distributed(x, 15, shard_fn=_oracle_shard, stats=st)
         ei, ed = oracle.knn_exact(x, 15)
-        q.put((rank, bool(np.array_equal(idx, ei) and np.array_equal(d, ed))))
+        # each rank sends only its owned rows' records (300 rows x (1 + 2 * 15) int32 + the count), not the
+        # full n x k' arrays
+        small = st["bytes_sent"] <= 300 * 31 * 4 + 8
+        q.put((rank, bool(np.array_equal(idx, ei) and np.array_equal(d, ed) and small)))
     finally:
         dist.destroy_process_group()
 
