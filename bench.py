@@ -5,7 +5,8 @@
 
 A learned initialiser (MLP 128-512-512-2) is first trained, outside the timed region, on the plain GPU
 embedding of 200,000 draws of the generator. One step = one full learned-init fit_transform of a fresh
-draw (preprocess -> exact kNN -> reselection -> MN/FP sampling -> MLP prediction as Value init -> CSR ->
+draw (preprocess -> exact kNN -> reselection -> MN/FP sampling -> MLP prediction in the training
+embedding's coordinates as the start -> CSR ->
 the shortened schedule (0, 50, 150) of fused gradient+Adam iterations in one CUDA graph):
   * value: inputs resident in HBM, C ABI `pacmap_fit_transform_learned_device`, CUDA events around
            each step; the plain schedule (Random init, (100, 100, 250)) on the same draw is timed the
@@ -282,7 +283,7 @@ def run_ours(args, rank, world, local_rank):
     n_train = min(w["n_train"], max(n // 5, 4096))
     # the learned initialiser is trained once per generator (outside the timed region): plain GPU PaCMAP
     # of n_train draws, then AdamW on (x', embedding)
-    train_s, train_losses, train_fit_s = None, None, None
+    train_s, train_losses, train_fit_s, tstats = None, None, None, None
     if args.minimal:
         params = learned.init_params(d, dim, seed=0)
     else:
@@ -298,6 +299,8 @@ def run_ours(args, rank, world, local_rank):
         params, train_losses = learned.train(learned.init_params(d, dim, seed=0), xp_train, y_train, epochs=20,
                                              batch=4096, lr=1e-3, weight_decay=1e-4, seed=0, device=local_rank)
         train_s = time.perf_counter() - t0
+        # the fits start from the prediction in the training embedding's coordinates
+        tstats = learned.target_stats(y_train)
         del x_train, y_train, xp_train
     # a fresh draw of the same generator
     x = make_data(n, d, seed=0, draw_seed=1000 + rank, generator=gen)
@@ -315,10 +318,11 @@ def run_ours(args, rank, world, local_rank):
     gate = {"continued": False}
 
     def step_learned():
-        learned.fit_transform_learned_device(dx.data_ptr(), n, d, dy_l.data_ptr(), params, cfg_short)
+        learned.fit_transform_learned_device(dx.data_ptr(), n, d, dy_l.data_ptr(), params, cfg_short,
+                                             target_stats=tstats)
         if gate["continued"]:
-            # the run missed the plain run's 10-NN preservation by more than 0.005: continue it on the
-            # plain schedule from where it stopped
+            # the run missed the plain run's quality by more than 0.005: continue it on the plain schedule
+            # from where it stopped
             cont = pm.Configuration(initialization=pm.Initialization.Value(dy_l.cpu().numpy()), seed=7,
                                     embedding_dimensions=dim, device=local_rank)
             pm.fit_transform_device(dx.data_ptr(), n, d, dy_c.data_ptr(), cont)
@@ -329,9 +333,10 @@ def run_ours(args, rank, world, local_rank):
     def step_e2e():
         cc = pm._CConfig(cfg_short, n)
         p = np.ascontiguousarray(params, dtype=np.float32)
+        tm_, ts_ = (None, None) if tstats is None else (C.c_void_p(tstats[0].ctypes.data), C.c_void_p(tstats[1].ctypes.data))
         pm._check(_abi.lib().pacmap_fit_transform_learned(C.c_void_p(hx.data_ptr()), n, d, C.byref(cc.c),
-                                                          C.c_void_p(p.ctypes.data), C.c_void_p(hy.data_ptr()),
-                                                          None))
+                                                          C.c_void_p(p.ctypes.data), tm_, ts_,
+                                                          C.c_void_p(hy.data_ptr()), None))
 
     def barrier():
         if dist:
@@ -388,7 +393,7 @@ def run_ours(args, rank, world, local_rank):
     pm.set_stage_timing(True)
     step_plain()
     stages_plain = pm.stage_times()
-    learned.fit_transform_learned_device(dx.data_ptr(), n, d, dy_l.data_ptr(), params, cfg_short)
+    learned.fit_transform_learned_device(dx.data_ptr(), n, d, dy_l.data_ptr(), params, cfg_short, target_stats=tstats)
     stages_learned = pm.stage_times()
     pm.set_stage_timing(False)
 
@@ -444,7 +449,7 @@ def run_ours(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": (f"learned-init PaCMAP of a fresh {n}x{d} draw -> {dim}-D: MLP {d}-512-512-{dim} "
-                                f"prediction as Value init + schedule {learned.SHORT_SCHEDULE}; vs plain Random(7) "
+                                f"prediction (in the training embedding's coordinates) as the start + schedule {learned.SHORT_SCHEDULE}; vs plain Random(7) "
                                 f"with {learned.PLAIN_SCHEDULE}; exact kNN (k'={min(_pair_counts(n)[0] + 50, n - 1)})"),
                    "n": n, "d": d, "dim": dim, "generator": w["generator_desc"],
                    "mlp_training": f"{n_train} draws (draw seed 10000+rank), plain GPU embedding, 20 epochs, batch "

@@ -238,12 +238,18 @@ pacmap_status pacmap_mlp_apply(const float* params, uint64_t d, uint64_t dim, co
  * parameter layout, out_loss the loss (the check against a CPU oracle). */
 pacmap_status pacmap_mlp_grad(const float* params, uint64_t d, uint64_t dim, const float* xp, const float* target,
                               uint64_t batch, int32_t device, float* out_grads, float* out_loss);
-/* fit_transform (src/lib.rs:294-367) with the learned initialiser: the embedding starts from MLP(x')
- * through Initialization::Value; cfg->init_kind is ignored. Use a shortened cfg->num_iters. */
+/* fit_transform (src/lib.rs:294-367) with the learned initialiser; cfg->init_kind is ignored, pass a
+ * shortened cfg->num_iters. target_mean, target_std (dim values each, host; see pacmap_model_target_stats):
+ * the training embedding's per-dimension mean and std -- given, the fit starts from MLP(x') * std + mean,
+ * the training embedding's coordinates (where pacmap_transform places new points), so the predicted
+ * layout survives the first Adam steps; NULL (both), it starts from MLP(x') through Initialization::Value
+ * (src/lib.rs:753-766: z-scored to std 1e-4 like any Value init). */
 pacmap_status pacmap_fit_transform_learned(const float* x, uint64_t n, uint64_t d, const pacmap_config* cfg,
-                                           const float* mlp_params, float* out_embedding, float* out_snapshots);
+                                           const float* mlp_params, const float* target_mean, const float* target_std,
+                                           float* out_embedding, float* out_snapshots);
 pacmap_status pacmap_fit_transform_learned_device(const float* d_x, uint64_t n, uint64_t d, const pacmap_config* cfg,
-                                                  const float* mlp_params, float* d_out_embedding,
+                                                  const float* mlp_params, const float* target_mean,
+                                                  const float* target_std, float* d_out_embedding,
                                                   float* d_out_snapshots);
 
 /* Initialization::Pca's eigen-step on the host (no GPU): the k leading eigenvectors of a symmetric

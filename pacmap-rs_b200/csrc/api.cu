@@ -242,7 +242,8 @@ uint64_t preprocess_for(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const 
 
 // fit_transform with x already on the device; h_* pointers are the caller's host views of the config.
 void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const pacmap_config& cfg, float* d_out,
-                        float* d_snap, const float* mlp_params = nullptr) {
+                        float* d_snap, const float* mlp_params = nullptr, const float* t_mean = nullptr,
+                        const float* t_std = nullptr) {
   // lib.rs:300-302
   PM_REQUIRE(n > 1, PACMAP_ERR_SAMPLE_SIZE, "Sample size must be larger than one");
   const uint64_t dim = cfg.embedding_dimensions;
@@ -290,7 +291,12 @@ void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const 
   if (dim == 0) return;
   // lib.rs:752-779 initial embedding
   tm.start(ST_INIT);
-  if (mlp_params) {
+  if (mlp_params && t_mean && t_std) {
+    // learned initialiser in the training embedding's coordinates: MLP(x') * std + mean, where the plain
+    // schedule would have placed the points (the network predicts standardised coordinates)
+    mlp_apply_device(c, mlp_params, d, dim, xp.get(), n, d_out);
+    destandardise_device(c, d_out, n, dim, t_mean, t_std);
+  } else if (mlp_params) {
     // learned initialiser: MLP(x') as Initialization::Value (lib.rs:753-766 z-scores it to std 1e-4)
     DevBuf<float> raw(c, n * dim);
     mlp_apply_device(c, mlp_params, d, dim, xp.get(), n, raw.get());
@@ -437,7 +443,8 @@ pacmap_status pacmap_fit_transform_device(const float* d_x, uint64_t n, uint64_t
 }
 
 pacmap_status pacmap_fit_transform_learned(const float* x, uint64_t n, uint64_t d, const pacmap_config* cfg,
-                                           const float* mlp_params, float* out_embedding, float* out_snapshots) {
+                                           const float* mlp_params, const float* target_mean, const float* target_std,
+                                           float* out_embedding, float* out_snapshots) {
   return guarded([&] {
     validate_config(cfg);
     PM_REQUIRE(n > 1, PACMAP_ERR_SAMPLE_SIZE, "Sample size must be larger than one");
@@ -449,7 +456,10 @@ pacmap_status pacmap_fit_transform_learned(const float* x, uint64_t n, uint64_t 
     upload(c, dx, x, n * d);
     const bool snaps = out_snapshots && cfg->snapshots && cfg->n_snapshots > 0;
     if (snaps) ds.alloc(c, cfg->n_snapshots * n * dim);
-    fit_transform_impl(c, dx.get(), n, d, *cfg, dy.get(), snaps ? ds.get() : nullptr, mlp_params);
+    PM_REQUIRE((target_mean == nullptr) == (target_std == nullptr), PACMAP_ERR_INVALID_ARGUMENT,
+               "target_mean and target_std go together");
+    fit_transform_impl(c, dx.get(), n, d, *cfg, dy.get(), snaps ? ds.get() : nullptr, mlp_params, target_mean,
+                       target_std);
     PM_CUDA(cudaMemcpyAsync(out_embedding, dy.get(), n * dim * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
     if (snaps) PM_CUDA(cudaMemcpyAsync(out_snapshots, ds.get(), ds.bytes(), cudaMemcpyDeviceToHost, c.stream));
     PM_CUDA(cudaStreamSynchronize(c.stream));
@@ -457,14 +467,18 @@ pacmap_status pacmap_fit_transform_learned(const float* x, uint64_t n, uint64_t 
 }
 
 pacmap_status pacmap_fit_transform_learned_device(const float* d_x, uint64_t n, uint64_t d, const pacmap_config* cfg,
-                                                  const float* mlp_params, float* d_out_embedding,
+                                                  const float* mlp_params, const float* target_mean,
+                                                  const float* target_std, float* d_out_embedding,
                                                   float* d_out_snapshots) {
   return guarded([&] {
     validate_config(cfg);
     PM_REQUIRE(n > 1, PACMAP_ERR_SAMPLE_SIZE, "Sample size must be larger than one");
     PM_REQUIRE(d_x && mlp_params && d_out_embedding, PACMAP_ERR_INVALID_ARGUMENT, "NULL buffer");
     DeviceLock dl(cfg->device);
-    fit_transform_impl(dl.ctx, d_x, n, d, *cfg, d_out_embedding, d_out_snapshots, mlp_params);
+    PM_REQUIRE((target_mean == nullptr) == (target_std == nullptr), PACMAP_ERR_INVALID_ARGUMENT,
+               "target_mean and target_std go together");
+    fit_transform_impl(dl.ctx, d_x, n, d, *cfg, d_out_embedding, d_out_snapshots, mlp_params, target_mean,
+                       target_std);
     PM_CUDA(cudaStreamSynchronize(dl.ctx.stream));
   });
 }

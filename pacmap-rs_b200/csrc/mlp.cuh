@@ -24,6 +24,8 @@ void model_save(const char* path, uint64_t d, uint64_t dim, const float* params,
 void model_load(const char* path, uint64_t* d, uint64_t* dim, float* params, float* pre_min, float* pre_max,
                 float* pre_mean, float* t_mean, float* t_std);
 // out (n x dim, device) = MLP((x - min) / max - mean) * std + mean_t for device x (n x d); host constants.
+// y = y * t_std + t_mean per dimension (host vectors of dim values), in place on the device.
+void destandardise_device(Ctx& c, float* d_y, uint64_t n, uint64_t dim, const float* t_mean, const float* t_std);
 void transform_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t dim, const float* params,
                       float pre_min, float pre_max, const float* pre_mean, const float* t_mean, const float* t_std,
                       float* d_out);

@@ -164,6 +164,19 @@ void model_load(const char* path, uint64_t* d_out, uint64_t* dim_out, float* par
   r.get_f32(params, count);
 }
 
+void destandardise_device(Ctx& c, float* d_y, uint64_t n, uint64_t dim, const float* t_mean, const float* t_std) {
+  std::vector<float> ms(2 * dim);
+  for (uint64_t k = 0; k < dim; ++k) {
+    ms[k] = t_mean[k];
+    ms[dim + k] = t_std[k];
+  }
+  DevBuf<float> dms;
+  upload(c, dms, ms.data(), 2 * dim);
+  const unsigned g = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n * dim, 256), c.sm_count * 16ull));
+  destandardise_kernel<<<g, 256, 0, c.stream>>>(d_y, n, dim, dms.get());
+  PM_LAUNCHED();
+}
+
 void transform_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t dim, const float* params,
                       float pre_min, float pre_max, const float* pre_mean, const float* t_mean, const float* t_std,
                       float* d_out) {

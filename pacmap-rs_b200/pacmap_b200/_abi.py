@@ -70,8 +70,9 @@ _SIGS = {
     "pacmap_mlp_train": (C.c_int, [_vp, _vp, _u64, _u64, _u64, _u64, _u64, _f32, _f32, _u64, _i32, _vp, _vp]),
     "pacmap_mlp_apply": (C.c_int, [_vp, _u64, _u64, _vp, _u64, _i32, _vp]),
     "pacmap_mlp_grad": (C.c_int, [_vp, _u64, _u64, _vp, _vp, _u64, _i32, _vp, _vp]),
-    "pacmap_fit_transform_learned": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp, _vp]),
-    "pacmap_fit_transform_learned_device": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp, _vp]),
+    "pacmap_fit_transform_learned": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp, _vp, _vp, _vp]),
+    "pacmap_fit_transform_learned_device": (C.c_int, [_vp, _u64, _u64, C.POINTER(Config), _vp, _vp, _vp, _vp,
+                                                      _vp]),
     "pacmap_pca_axes": (C.c_int, [_vp, _u64, _u64, _vp]),
     "pacmap_model_target_stats": (C.c_int, [_vp, _u64, _u64, _vp, _vp]),
     "pacmap_model_save": (C.c_int, [C.c_char_p, _u64, _u64, _vp, _f32, _f32, _vp, _vp, _vp]),

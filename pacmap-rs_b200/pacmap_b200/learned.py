@@ -79,9 +79,19 @@ def gradient(params, xp, target, device: int = 0):
     return loss.value, g
 
 
-def fit_transform_learned(x, params, config: Optional[Configuration] = None):
-    """fit_transform (lib.rs:294-367) starting from MLP(x') through Initialization::Value.
+def _stats_ptrs(target_stats):
+    if target_stats is None:
+        return None, None, ()
+    mean, std = (np.ascontiguousarray(v, dtype=np.float32) for v in target_stats)
+    return ptr(mean), ptr(std), (mean, std)
 
+
+def fit_transform_learned(x, params, config: Optional[Configuration] = None, target_stats=None):
+    """fit_transform (lib.rs:294-367) starting from the network's prediction.
+
+    ``target_stats`` = (mean, std) of the training embedding (``target_stats(y_train)``): the fit starts from
+    MLP(x') in that embedding's coordinates, so the predicted layout survives the first Adam steps. Without
+    it, from MLP(x') through Initialization::Value (z-scored to std 1e-4, lib.rs:753-766).
     ``config.initialization`` is ignored; pass a shortened ``num_iters`` (``SHORT_SCHEDULE``)."""
     config = config or dataclasses.replace(Configuration(), num_iters=SHORT_SCHEDULE)
     x = np.ascontiguousarray(x, dtype=np.float32)
@@ -93,16 +103,19 @@ def fit_transform_learned(x, params, config: Optional[Configuration] = None):
     snaps = None
     if config.snapshots is not None:
         snaps = np.zeros((len(config.snapshots), n, dim), np.float32)
-    _check(_abi.lib().pacmap_fit_transform_learned(ptr(x), n, d, C.byref(cc.c), ptr(p), ptr(out), ptr(snaps)))
+    pm_, ps_, _keep = _stats_ptrs(target_stats)
+    _check(_abi.lib().pacmap_fit_transform_learned(ptr(x), n, d, C.byref(cc.c), ptr(p), pm_, ps_, ptr(out),
+                                                   ptr(snaps)))
     return out, snaps
 
 
 def fit_transform_learned_device(x_ptr: int, n: int, d: int, out_ptr: int, params, config: Configuration,
-                                 snapshots_ptr: Optional[int] = None) -> None:
-    """fit_transform_learned on device memory (raw CUDA pointers); params stay a host array."""
+                                 snapshots_ptr: Optional[int] = None, target_stats=None) -> None:
+    """fit_transform_learned on device memory (raw CUDA pointers); params and target_stats stay host arrays."""
     p = np.ascontiguousarray(params, dtype=np.float32)
     cc = _CConfig(dataclasses.replace(config, initialization=Initialization.Random(0)), n)
-    _check(_abi.lib().pacmap_fit_transform_learned_device(C.c_void_p(x_ptr), n, d, C.byref(cc.c), ptr(p),
+    pm_, ps_, _keep = _stats_ptrs(target_stats)
+    _check(_abi.lib().pacmap_fit_transform_learned_device(C.c_void_p(x_ptr), n, d, C.byref(cc.c), ptr(p), pm_, ps_,
                                                           C.c_void_p(out_ptr),
                                                           C.c_void_p(snapshots_ptr) if snapshots_ptr else None))
 

@@ -121,12 +121,31 @@ def test_learned_init_gains_over_random_init_on_the_short_schedule(lib):
     short = lib.Configuration(seed=1, num_iters=lib.learned.SHORT_SCHEDULE, initialization=lib.Initialization.Random(7))
     y_short, _ = lib.fit_transform(x_new, short)
     y_learned, _ = lib.learned.fit_transform_learned(x_new, p, short)
+    y_scaled, _ = lib.learned.fit_transform_learned(x_new, p, short, target_stats=lib.learned.target_stats(y_train))
     q_plain = lib.quality(x_new, y_plain, sample, trip)
     q_short = lib.quality(x_new, y_short, sample, trip)
     q_learned = lib.quality(x_new, y_learned, sample, trip)
-    print(f"plain {q_plain}, random+short {q_short}, learned+short {q_learned}")
+    q_scaled = lib.quality(x_new, y_scaled, sample, trip)
+    print(f"plain {q_plain}, random+short {q_short}, learned+short {q_learned}, learned (own scale)+short {q_scaled}")
     assert q_learned[0] >= q_plain[0] - 0.005
     assert q_learned[1] >= q_short[1] + 0.02
+    # started in the training embedding's coordinates, the short schedule keeps the predicted layout: both
+    # metrics within 0.005 of the plain schedule
+    assert q_scaled[0] >= q_plain[0] - 0.005 and q_scaled[1] >= q_plain[1] - 0.005
+
+
+def test_learned_start_in_training_coordinates_is_the_destandardised_prediction(lib):
+    # with target statistics the fit starts from MLP(x') * std + mean: zero iterations return exactly that
+    from pacmap_b200 import datasets
+
+    x, _ = datasets.anisotropic_mixture(3000, 32, 6, seed=2)
+    p = lib.learned.init_params(32, 2, seed=4)
+    mean, std = np.array([3.0, -2.0], np.float32), np.array([10.0, 20.0], np.float32)
+    y0, _ = lib.learned.fit_transform_learned(x, p, lib.Configuration(seed=3, num_iters=(0, 0, 0)),
+                                              target_stats=(mean, std))
+    xp, *_ = lib.stages.preprocess(x)
+    z = lib.learned.apply(p, xp, 2)
+    assert np.array_equal(y0, (z * std + mean).astype(np.float32))
 
 
 def test_transform_is_the_training_preprocessing_the_network_and_the_embedding_scale(lib, tmp_path):
