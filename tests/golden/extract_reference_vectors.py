@@ -1,7 +1,9 @@
 """Extract the golden vectors of the reference's own unit tests into ``reference_vectors.json``.
 
-Run in a container where the reference checkout is mounted (default ``/root/reference``; override with
-``PACMAP_REFERENCE``). The tests never read the reference at run time: they use the committed JSON.
+    python tests/golden/extract_reference_vectors.py <path of the reference checkout>
+
+(or set ``PACMAP_REFERENCE`` to that path). The tests never read the reference at run time: they use the
+committed JSON.
 
 Sources (beamform/pacmap-rs v0.2.6):
   * src/gradient.rs:162-195  test_pacmap_grad: y, pairs, weights -> 11x2 gradient incl. loss;
@@ -17,11 +19,13 @@ import os
 import re
 import sys
 
-REF = os.environ.get("PACMAP_REFERENCE", "/root/reference")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PACMAP_REFERENCE", "")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
 
 
 def _read(rel: str) -> str:
+    if not REF:
+        raise SystemExit("give the reference checkout's path as the first argument (or in PACMAP_REFERENCE)")
     with open(os.path.join(REF, rel)) as f:
         return f.read()
 
