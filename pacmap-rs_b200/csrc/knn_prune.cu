@@ -326,7 +326,123 @@ __global__ void __launch_bounds__(128) fill_tile_lists_kernel(const uint32_t* __
   }
 }
 
+// near[p * probe + r]: the `probe` pivots nearest pivot p, itself first, by f32 squared distance of the
+// pivot rows, ties to the lower index. One block per pivot, one thread per other pivot.
+__global__ void __launch_bounds__(PIV) pivot_near_kernel(const float* __restrict__ x,
+                                                         const uint32_t* __restrict__ piv_rows, int d, int probe,
+                                                         uint32_t* __restrict__ near) {
+  __shared__ uint64_t best[PIV / 32];
+  const int p = blockIdx.x, q = threadIdx.x, warp = q >> 5, lane = q & 31;
+  const float* xp = x + static_cast<uint64_t>(piv_rows[p]) * d;
+  const float* xq = x + static_cast<uint64_t>(piv_rows[q]) * d;
+  float acc = 0.0f;
+  for (int k = 0; k < d; ++k) {
+    const float df = xp[k] - xq[k];
+    acc = fmaf(df, df, acc);
+  }
+  uint64_t key = q == p ? 0ull : ((static_cast<uint64_t>(total_key(acc)) << 32) | static_cast<uint32_t>(q));
+  for (int r = 0; r < probe; ++r) {
+    uint64_t m = key;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const uint64_t t = __shfl_xor_sync(0xFFFFFFFFu, m, o);
+      m = t < m ? t : m;
+    }
+    if (lane == 0) best[warp] = m;
+    __syncthreads();
+    uint64_t b = best[0];
+    for (int w = 1; w < PIV / 32; ++w) b = best[w] < b ? best[w] : b;
+    const int winner = b == 0ull ? p : static_cast<int>(b & 0xFFFFFFFFu);
+    if (q == 0) near[p * probe + r] = static_cast<uint32_t>(winner);
+    if (q == winner) key = ~0ull;
+    __syncthreads();
+  }
+}
+
+// Per row block: the column tiles of its own cells, then those of the probe - 1 cells nearest each of its
+// own cells (ascending tile order in each group, no repeats). Count pass (list == nullptr) or fill pass.
+constexpr int PL_MAX_WORDS = 4096;  // tile bitmask words in shared memory (ntiles <= 131,072)
+__global__ void __launch_bounds__(PIV) probe_lists_kernel(const uint32_t* __restrict__ cstart, uint64_t n, int ntiles,
+                                                          const uint32_t* __restrict__ near, int probe, int blk0,
+                                                          const uint32_t* __restrict__ ptr,
+                                                          uint32_t* __restrict__ counts, uint32_t* __restrict__ list) {
+  __shared__ uint32_t own[PL_MAX_WORDS], other[PL_MAX_WORDS];
+  __shared__ uint32_t wsum[PIV / 32];
+  const int words = (ntiles + 31) / 32;
+  const int b = static_cast<int>(blockIdx.x) + blk0, p = threadIdx.x;
+  for (int w = p; w < words; w += PIV) own[w] = other[w] = 0u;
+  __syncthreads();
+  const uint64_t r0 = static_cast<uint64_t>(b) * TC_BM, r1 = min(r0 + TC_BM, n);
+  auto mark = [&](uint32_t* mask, int q) {
+    const uint32_t a = cstart[q], e = q + 1 < PIV ? cstart[q + 1] : static_cast<uint32_t>(n);
+    if (e <= a) return;
+    for (uint32_t t = a / TC_BN; t <= (e - 1) / TC_BN; ++t) atomicOr(&mask[t >> 5], 1u << (t & 31));
+  };
+  const uint32_t a = cstart[p], e = p + 1 < PIV ? cstart[p + 1] : static_cast<uint32_t>(n);
+  const bool mine = r0 < r1 && a < r1 && e > r0;
+  if (mine) mark(own, p);
+  __syncthreads();
+  if (mine)
+    for (int r = 1; r < probe; ++r) mark(other, static_cast<int>(near[p * probe + r]));
+  __syncthreads();
+  uint32_t c = 0;
+  for (int w = p; w < words; w += PIV) {
+    other[w] &= ~own[w];
+    c += __popc(own[w]) + __popc(other[w]);
+  }
+  c = __reduce_add_sync(0xFFFFFFFFu, c);
+  if ((p & 31) == 0) wsum[p >> 5] = c;
+  __syncthreads();
+  if (!list) {
+    if (p == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < PIV / 32; ++w) t += wsum[w];
+      counts[b] = t;
+    }
+    return;
+  }
+  if (p == 0) {
+    uint32_t pos = ptr[b];
+    for (int g = 0; g < 2; ++g) {
+      const uint32_t* mask = g == 0 ? own : other;
+      for (int w = 0; w < words; ++w)
+        for (uint32_t m = mask[w]; m; m &= m - 1) list[pos++] = static_cast<uint32_t>(w * 32 + __ffs(m) - 1);
+    }
+  }
+}
+
 }  // namespace
+
+uint64_t build_probe_tile_lists(Ctx& c, const float* d_x, uint64_t d, const uint32_t* d_piv_rows,
+                                const uint32_t* d_cstart, uint64_t n, uint64_t n_pad, int probe, uint64_t blk0,
+                                uint64_t blk1, DevBuf<uint32_t>& ptr, DevBuf<uint32_t>& list) {
+  const uint64_t nb = n_pad / TC_BM, ntiles = n_pad / TC_BN;
+  PM_REQUIRE((ntiles + 31) / 32 <= static_cast<uint64_t>(PL_MAX_WORDS) && probe >= 1 && probe <= PIV,
+             PACMAP_ERR_UNSUPPORTED, "probe lists: too many tiles");
+  DevBuf<uint32_t> near(c, static_cast<uint64_t>(PIV) * probe), counts(c, nb);
+  pivot_near_kernel<<<PIV, PIV, 0, c.stream>>>(d_x, d_piv_rows, static_cast<int>(d), probe, near.get());
+  PM_LAUNCHED();
+  PM_CUDA(cudaMemsetAsync(counts.get(), 0, nb * sizeof(uint32_t), c.stream));
+  const unsigned nblk = static_cast<unsigned>(blk1 - blk0);
+  if (nblk) {
+    probe_lists_kernel<<<nblk, PIV, 0, c.stream>>>(d_cstart, n, static_cast<int>(ntiles), near.get(), probe,
+                                                   static_cast<int>(blk0), nullptr, counts.get(), nullptr);
+    PM_LAUNCHED();
+  }
+  ptr.alloc(c, nb + 1);
+  scan_counts_kernel<<<1, 1024, 0, c.stream>>>(counts.get(), nb, ptr.get());
+  PM_LAUNCHED();
+  uint32_t total = 0;
+  PM_CUDA(cudaMemcpyAsync(&total, ptr.get() + nb, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+  PM_CUDA(cudaStreamSynchronize(c.stream));
+  list.alloc(c, std::max<uint64_t>(total, 1));
+  if (nblk) {
+    probe_lists_kernel<<<nblk, PIV, 0, c.stream>>>(d_cstart, n, static_cast<int>(ntiles), near.get(), probe,
+                                                   static_cast<int>(blk0), ptr.get(), counts.get(), list.get());
+    PM_LAUNCHED();
+  }
+  return total;
+}
 
 void select_pivots(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint32_t* d_piv_rows) {
   const uint32_t S = static_cast<uint32_t>(std::min<uint64_t>(n, PV_SUB_MAX));

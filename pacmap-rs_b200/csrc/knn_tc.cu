@@ -972,7 +972,12 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   // Tile lists over the cells nearest each row block: every row block visits only the column tiles of
   // the `probe` pivot cells whose pivots are nearest its own cells' (own cells first). The cells are
   // contiguous ranges of the locality order: cell p starts at the first chunk's offset for p.
-  auto probe_lists = [&](int probe, DevBuf<uint32_t>& tile_ptr, DevBuf<uint32_t>& tile_list) {
+  const uint64_t blocks_all = nblocks;
+  const uint64_t sblk0 = blocks_all * shard.index / shard.count, sblk1 = blocks_all * (shard.index + 1) / shard.count;
+  auto probe_lists = [&](int probe, DevBuf<uint32_t>& tile_ptr, DevBuf<uint32_t>& tile_list) -> uint64_t {
+    if (ntl <= 131072)  // on the device: the cell starts are the first chunk's offsets
+      return build_probe_tile_lists(c, d_x, d, piv_rows.get(), cell_counts.get(), n, n_pad, probe, sblk0, sblk1,
+                                    tile_ptr, tile_list);
     std::vector<uint32_t> cstart(PIV + 1);
     DevBuf<float> piv(c, static_cast<uint64_t>(PIV) * d);
     gather_pivots_kernel<<<PIV, 128, 0, c.stream>>>(d_x, piv_rows.get(), static_cast<int>(d), piv.get());
@@ -1021,7 +1026,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     if (list.empty()) list.push_back(0);
     upload(c, tile_ptr, ptr.data(), ptr.size());
     upload(c, tile_list, list.data(), list.size());
-    return ptr;
+    return static_cast<uint64_t>(ptr[sblk1] - ptr[sblk0]);
   };
 
   DevBuf<uint32_t> tile_ptr, tile_list;
@@ -1142,8 +1147,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     // First pass: each block over the cells nearest its own gives every row a bound of its k'-th
     // neighbour distance; then the tiles that may hold a neighbour of some row of the block.
     DevBuf<uint32_t> aptr, alist, aovf(c, n + 1);
-    const std::vector<uint32_t> hptr = probe_lists(PRUNE_PROBE, aptr, alist);
-    st.tiles_bound = hptr[blk1] - hptr[blk0];
+    st.tiles_bound = probe_lists(PRUNE_PROBE, aptr, alist);
     PM_CUDA(cudaMemsetAsync(aovf.get() + n, 0, sizeof(uint32_t), c.stream));
     run_filter(aptr.get(), alist.get(), aovf.get(), aovf.get() + n);
     c.check_errors("tensor-core kNN bound pass");
