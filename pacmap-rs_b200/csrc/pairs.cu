@@ -265,14 +265,15 @@ __device__ __forceinline__ float group8_ref_dist(const float* __restrict__ a, co
   return __fsqrt_rn(t);
 }
 
-__global__ void sample_mn_kernel(const float* __restrict__ x, uint64_t n, int d, uint32_t n_mn, uint64_t seed,
-                                 uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
-  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+// The mid-near pairs of point i by the reference's sequential rule (one warp; picks kept in `out`).
+__device__ __noinline__ void mn_point_sequential(const float* __restrict__ x, uint64_t n, int d, uint32_t n_mn,
+                                                 uint64_t seed, uint64_t i, uint32_t* __restrict__ out,
+                                                 uint32_t* __restrict__ err) {
   const uint32_t lane = lane_id();
   const int l8 = lane & 7;
   const unsigned gbase = lane & ~7u;
   const int grp = lane >> 3;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+  {
     uint32_t* picks = out + (i * n_mn) * 2 + 1;
     PointStream s(seed, i);
     uint64_t budget = SAMPLE_ATTEMPT_CAP;
@@ -350,6 +351,158 @@ __global__ void sample_mn_kernel(const float* __restrict__ x, uint64_t n, int d,
       }
       __syncwarp();
     }
+  }
+}
+
+__global__ void sample_mn_kernel(const float* __restrict__ x, uint64_t n, int d, uint32_t n_mn, uint64_t seed,
+                                 uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps)
+    mn_point_sequential(x, n, d, n_mn, seed, i, out, err);
+}
+
+// Speculative mid-near sampling (sampling.rs:118-142, 296-313), one warp per point, n_mn <= 32 and
+// n >= n_mn + 7 (every slot then draws 6 candidates). The draws of every slot are made first, with the
+// exclusion of the earlier slots' picks left out; then the 6 * n_mn candidate rows are gathered with many
+// loads in flight (4 groups of 8 lanes, two rows each per pass; row i in NC registers per lane), each
+// slot takes its 2nd-closest candidate, and the draws are checked: when no candidate of slot j is the
+// pick of an earlier slot, the sequential rule would have accepted and rejected exactly the same stream
+// words, so the picks are the rule's picks. Otherwise (rare: about 120 * n_mn / n per point) the point
+// is redone by the sequential rule. Candidates and distances are staged in shared memory.
+constexpr int MS_WARPS = 8, MS_MAXC = 32 * 6;
+template <int NC>
+__global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_spec_kernel(const float* __restrict__ x, uint64_t n, int d,
+                                                                      uint32_t n_mn, uint64_t seed,
+                                                                      uint32_t* __restrict__ out,
+                                                                      uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_cand[MS_WARPS][MS_MAXC];
+  __shared__ float s_dist[MS_WARPS][MS_MAXC];
+  const int warp = threadIdx.x >> 5;
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * MS_WARPS;
+  const uint32_t lane = lane_id();
+  const int l8 = lane & 7;
+  const unsigned gbase = lane & ~7u;
+  const int grp = lane >> 3;
+  const int nc = d >> 3;
+  const int total = static_cast<int>(n_mn) * 6;
+  uint32_t* cs = s_cand[warp];
+  float* ds = s_dist[warp];
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * MS_WARPS + warp; i < n; i += warps) {
+    // 1. every slot's draws (self and repeats within the slot rejected, as in the rule)
+    WarpStream s(seed, i);
+    uint64_t budget = SAMPLE_ATTEMPT_CAP;
+    bool failed = false;
+    for (uint32_t jslot = 0; jslot < n_mn && !failed; ++jslot) {
+      uint32_t cand[6] = {0, 0, 0, 0, 0, 0};
+      uint32_t cnt = 0;
+      while (cnt < 6) {
+        uint32_t j;
+        if (!s.uniform(static_cast<uint32_t>(n), j, budget)) {
+          failed = true;
+          break;
+        }
+        if (j == i) continue;
+        bool dup = false;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) dup |= (t < static_cast<int>(cnt) && cand[t] == j);
+        if (dup) continue;
+#pragma unroll
+        for (int t = 0; t < 6; ++t)
+          if (t == static_cast<int>(cnt)) cand[t] = j;
+        ++cnt;
+      }
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (static_cast<int>(lane) == t) cs[jslot * 6 + t] = cand[t];
+    }
+    __syncwarp();
+    if (failed) {  // the sequential rule reports the failure
+      mn_point_sequential(x, n, d, n_mn, seed, i, out, err);
+      continue;
+    }
+    // 2. the reference's f32 distance of every candidate (distance.rs:50-75 order)
+    const float* a = x + i * d;
+    float ra[NC];
+#pragma unroll
+    for (int ch = 0; ch < NC; ++ch) ra[ch] = ch < nc ? a[8 * ch + l8] : 0.0f;
+    for (int c0 = 0; c0 < total; c0 += 8) {
+      const int ca = c0 + grp, cb = c0 + 4 + grp;
+      const uint32_t ja = ca < total ? cs[ca] : static_cast<uint32_t>(i);
+      const uint32_t jb = cb < total ? cs[cb] : static_cast<uint32_t>(i);
+      const float* pa = x + static_cast<uint64_t>(ja) * d;
+      const float* pb = x + static_cast<uint64_t>(jb) * d;
+      float va[NC], vb[NC];
+#pragma unroll
+      for (int ch = 0; ch < NC; ++ch) {
+        va[ch] = ch < nc ? pa[8 * ch + l8] : 0.0f;
+        vb[ch] = ch < nc ? pb[8 * ch + l8] : 0.0f;
+      }
+      float acc_a = 0.0f, acc_b = 0.0f;
+#pragma unroll
+      for (int ch = 0; ch < NC; ++ch) {
+        if (ch < nc) {
+          const float da = __fsub_rn(ra[ch], va[ch]), db = __fsub_rn(ra[ch], vb[ch]);
+          acc_a = __fadd_rn(acc_a, __fmul_rn(da, da));
+          acc_b = __fadd_rn(acc_b, __fmul_rn(db, db));
+        }
+      }
+      float ta = 0.0f, tb = 0.0f;
+#pragma unroll
+      for (int l = 0; l < 8; ++l) {
+        ta = __fadd_rn(ta, __shfl_sync(0xFFFFFFFFu, acc_a, gbase + l));
+        tb = __fadd_rn(tb, __shfl_sync(0xFFFFFFFFu, acc_b, gbase + l));
+      }
+      for (int e = nc * 8; e < d; ++e) {
+        const float da = __fsub_rn(a[e], pa[e]), db = __fsub_rn(a[e], pb[e]);
+        ta = __fadd_rn(ta, __fmul_rn(da, da));
+        tb = __fadd_rn(tb, __fmul_rn(db, db));
+      }
+      if (l8 == 0) {
+        if (ca < total) ds[ca] = __fsqrt_rn(ta);
+        if (cb < total) ds[cb] = __fsqrt_rn(tb);
+      }
+    }
+    __syncwarp();
+    // 3. lane j: slot j's 2nd smallest (distance key, draw order), then the check of its draws against the
+    //    picks of the earlier slots
+    uint32_t pick = 0;
+    if (lane < n_mn) {
+      uint64_t best0 = ~0ull, best1 = ~0ull;
+      uint32_t id0 = 0, id1 = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const uint32_t id = cs[lane * 6 + t];
+        const uint64_t key = (static_cast<uint64_t>(total_key(ds[lane * 6 + t])) << 3) | static_cast<uint64_t>(t);
+        if (key < best0) {
+          best1 = best0;
+          id1 = id0;
+          best0 = key;
+          id0 = id;
+        } else if (key < best1) {
+          best1 = key;
+          id1 = id;
+        }
+      }
+      pick = id1;
+    }
+    bool clash = false;
+    for (uint32_t q = 0; q + 1 < n_mn; ++q) {
+      const uint32_t pq = __shfl_sync(0xFFFFFFFFu, pick, q);
+      if (lane < n_mn && q < lane) {
+#pragma unroll
+        for (int t = 0; t < 6; ++t) clash |= cs[lane * 6 + t] == pq;
+      }
+    }
+    __syncwarp();
+    if (__any_sync(0xFFFFFFFFu, clash)) {
+      mn_point_sequential(x, n, d, n_mn, seed, i, out, err);
+      continue;
+    }
+    if (lane < n_mn) {
+      out[(i * n_mn + lane) * 2 + 0] = static_cast<uint32_t>(i);
+      out[(i * n_mn + lane) * 2 + 1] = pick;
+    }
+    __syncwarp();
   }
 }
 
@@ -523,7 +676,12 @@ void sample_mn_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, uint64_
   const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div(n, 8), c.sm_count * 32ull));
   const int di = static_cast<int>(d);
   const uint32_t m32 = static_cast<uint32_t>(n_mn);
-  if (n_mn <= 32 && d <= 128)
+  const bool spec = n_mn <= 32 && n >= n_mn + 7;
+  if (spec && d <= 128)
+    sample_mn_spec_kernel<16><<<grid, MS_WARPS * 32, 0, c.stream>>>(d_xp, n, di, m32, seed, d_pmn, c.d_err);
+  else if (spec && d <= 256)
+    sample_mn_spec_kernel<32><<<grid, MS_WARPS * 32, 0, c.stream>>>(d_xp, n, di, m32, seed, d_pmn, c.d_err);
+  else if (n_mn <= 32 && d <= 128)
     sample_mn_reg_kernel<16><<<grid, 256, 0, c.stream>>>(d_xp, n, di, m32, seed, d_pmn, c.d_err);
   else if (n_mn <= 32 && d <= 256)
     sample_mn_reg_kernel<32><<<grid, 256, 0, c.stream>>>(d_xp, n, di, m32, seed, d_pmn, c.d_err);
