@@ -223,8 +223,9 @@ __global__ void __launch_bounds__(256) prune_tiles_kernel(const int* __restrict_
                                                           const float* __restrict__ seg_rad,
                                                           const float* __restrict__ seg_ub,
                                                           const float* __restrict__ minT, uint64_t nseg, int ntiles,
-                                                          int words, int blk0, uint32_t* __restrict__ bits,
-                                                          uint32_t* __restrict__ counts) {
+                                                          int words, int blk0, const uint32_t* __restrict__ skip_ptr,
+                                                          const uint32_t* __restrict__ skip_list,
+                                                          uint32_t* __restrict__ bits, uint32_t* __restrict__ counts) {
   __shared__ float ms[2 * SEGS][PIV];
   __shared__ int sp[2 * SEGS];
   __shared__ float srad[2 * SEGS], sthr[2 * SEGS];
@@ -265,11 +266,19 @@ __global__ void __launch_bounds__(256) prune_tiles_kernel(const int* __restrict_
     }
     const unsigned bal = __ballot_sync(0xFFFFFFFFu, visit);
     const int word = (base >> 5) + warp;
-    if (lane == 0 && word < words) {
-      bits[static_cast<uint64_t>(blk) * words + word] = bal;
-      cnt += __popc(bal);
-    }
+    if (lane == 0 && word < words) bits[static_cast<uint64_t>(blk) * words + word] = bal;
   }
+  uint32_t* mine = bits + static_cast<uint64_t>(blk) * words;
+  if (skip_ptr) {
+    __syncthreads();
+    for (uint32_t e = skip_ptr[blk] + tid; e < skip_ptr[blk + 1]; e += blockDim.x) {
+      const uint32_t t = skip_list[e];
+      atomicAnd(&mine[t >> 5], ~(1u << (t & 31)));
+    }
+    __syncthreads();
+  }
+  for (int w = tid; w < words; w += blockDim.x) cnt += __popc(mine[w]);
+  cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
   if (lane == 0) wcount[warp] = cnt;
   __syncthreads();
   if (tid == 0) {
@@ -479,7 +488,7 @@ uint64_t build_pruned_tile_lists(Ctx& c, const PruneInputs& in, DevBuf<uint32_t>
   if (nblk) {
     prune_tiles_kernel<<<nblk, 256, 0, c.stream>>>(seg_cell.get(), seg_rad.get(), seg_ub.get(), minT.get(), nseg,
                                                    static_cast<int>(ntiles), words, static_cast<int>(in.blk0),
-                                                   bits.get(), counts.get());
+                                                   in.skip_ptr, in.skip_list, bits.get(), counts.get());
     PM_LAUNCHED();
   }
   ptr.alloc(c, nb + 1);

@@ -25,6 +25,9 @@ struct PruneInputs {
   uint64_t n = 0, n_pad = 0, d = 0;
   float inv_s = 1.0f;  // 1 / s (exact)
   uint64_t blk0 = 0, blk1 = 0;  // the row blocks to plan (a shard's range)
+  // tiles already computed for each row block (CSR, may be null): left out of the lists
+  const uint32_t* skip_ptr = nullptr;
+  const uint32_t* skip_list = nullptr;
 };
 
 // Per row block in [blk0, blk1): the column tiles of its own pivot cells, then those of the probe - 1
@@ -35,9 +38,9 @@ uint64_t build_probe_tile_lists(Ctx& c, const float* d_x, uint64_t d, const uint
                                 const uint32_t* d_cstart, uint64_t n, uint64_t n_pad, int probe, uint64_t blk0,
                                 uint64_t blk1, DevBuf<uint32_t>& ptr, DevBuf<uint32_t>& list);
 
-// Per row block in [blk0, blk1): the column tiles that may hold one of its rows' k' nearest points, in
-// the filter's sweep order, as a CSR list (ptr: n_pad / 256 + 1 offsets, list). Returns the number of
-// (block, tile) pairs kept.
+// Per row block in [blk0, blk1): the column tiles that may hold one of its rows' k' nearest points and are
+// not in its skip list, in the filter's sweep order, as a CSR list (ptr: n_pad / 256 + 1 offsets, list).
+// Returns the number of (block, tile) pairs kept.
 uint64_t build_pruned_tile_lists(Ctx& c, const PruneInputs& in, DevBuf<uint32_t>& ptr, DevBuf<uint32_t>& list);
 
 }  // namespace pacmap

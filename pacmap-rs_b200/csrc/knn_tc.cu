@@ -503,7 +503,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     int kb_rt, uint32_t idesc, const float2* __restrict__ ge, const float* __restrict__ nrm,
     const uint32_t* __restrict__ perm, int rank, uint2* __restrict__ cand, int* __restrict__ cand_cnt,
     uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err,
-    int block_offset, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_list) {
+    int block_offset, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_list,
+    const float* __restrict__ resume_theta) {
   using L = FilterLayout<KB, MODE>;
   constexpr int NST = L::NST;
   constexpr int C = 32 * PER;
@@ -690,6 +691,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const bool valid = row < n;
     float theta = valid ? 3.402823466e+38f : -__int_as_float(0x7f800000);
     int cnt = 0;
+    if (resume_theta && valid) {
+      // continue from an earlier pass over other tiles: its compacted buffer and threshold (an overflowed
+      // row stays overflowed; it is already listed for the exact fallback)
+      const int c0 = cand_cnt[row];
+      if (c0 < 0) {
+        theta = -__int_as_float(0x7f800000);
+      } else {
+        cnt = c0;
+        theta = resume_theta[row];
+      }
+    }
     const float n_i = valid ? nrm[row] : 0.0f;
     const float e4_i = valid ? ge[row].y : 0.0f;
     const uint64_t cbase = row * static_cast<uint64_t>(C);
@@ -791,7 +803,7 @@ constexpr int RC_WARPS = 4;
 template <int PER>
 __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     uint64_t n, int rank, const float* __restrict__ nrm, const float2* __restrict__ ge, uint2* __restrict__ cand,
-    int* __restrict__ cand_cnt, float* __restrict__ ub) {
+    int* __restrict__ cand_cnt, float* __restrict__ ub, float* __restrict__ theta_out) {
   constexpr int C = 32 * PER;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * RC_WARPS + warp; r < n;
@@ -799,6 +811,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     const int m0 = min(cand_cnt[r], C);
     if (m0 <= 0 || (ub && m0 < rank)) {
       if (ub && lane == 0) ub[r] = __int_as_float(0x7f800000);
+      if (theta_out && lane == 0) theta_out[r] = 3.402823466e+38f;  // every column met is still kept
       continue;
     }
     const uint64_t rb = r * static_cast<uint64_t>(C);
@@ -808,6 +821,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     const int m = warp_compact_regs<PER>(cand + rb, m0, min(rank, m0), n_i, e4_i, ge, th, &ukey);
     if (lane == 0) {
       cand_cnt[r] = m;
+      if (theta_out) theta_out[r] = th;
       if (ub) {
         // two f32 additions: within 2^-23 of the magnitudes summed (rounded up by 2^-22 of them)
         const float uk = key_to_float(ukey);
@@ -1097,14 +1111,15 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     }
   }
   // One filter launch over this shard's row blocks: with tile lists (ptr, list) or over every tile.
-  auto run_filter = [&](const uint32_t* lptr, const uint32_t* llist, uint32_t* ovf_rows, uint32_t* n_ovf) {
-    PM_CUDA(cudaMemsetAsync(ccnt.get(), 0xFF, n_pad * sizeof(int), c.stream));
+  auto run_filter = [&](const uint32_t* lptr, const uint32_t* llist, uint32_t* ovf_rows, uint32_t* n_ovf,
+                        const float* resume_theta) {
+    if (!resume_theta) PM_CUDA(cudaMemsetAsync(ccnt.get(), 0xFF, n_pad * sizeof(int), c.stream));
     auto launch = [&](auto kern, size_t smem) {
       PM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
       if (grid == 0) return;
       kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, KB, idesc, ge.get(), nrm.get(), perm.get(), rank,
                                                  cand.get(), ccnt.get(), ovf_rows, n_ovf, c.d_err,
-                                                 static_cast<int>(blk0), lptr, llist);
+                                                 static_cast<int>(blk0), lptr, llist, resume_theta);
     };
     const bool p16 = PER == 16;
     if (mode == MODE_STREAM) {
@@ -1131,11 +1146,13 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     PM_LAUNCHED();
   };
   const unsigned cgrid = std::min<unsigned>(ceil_div(n, RC_WARPS), c.sm_count * 16);
-  auto compact = [&](float* ub) {
+  auto compact = [&](float* ub, float* theta_out) {
     if (PER == 16)
-      knn_compact_kernel<16><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get(), ub);
+      knn_compact_kernel<16><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get(),
+                                                                    ub, theta_out);
     else
-      knn_compact_kernel<32><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get(), ub);
+      knn_compact_kernel<32><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get(),
+                                                                    ub, theta_out);
     PM_LAUNCHED();
   };
   cudaEvent_t ev[3];
@@ -1143,16 +1160,21 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   PM_CUDA(cudaEventRecord(ev[0], c.stream));
   st.tiles_full = static_cast<uint64_t>(grid) * ntl;
   st.tiles_visited = st.tiles_full;
+  PM_CUDA(cudaMemsetAsync(ovf.get() + n, 0, sizeof(uint32_t), c.stream));
+  PM_CUDA(cudaMemsetAsync(fbk.get() + n, 0, sizeof(uint32_t), c.stream));
+  DevBuf<uint32_t> aptr, alist;
+  DevBuf<float> resume;
   if (prune) {
     // First pass: each block over the cells nearest its own gives every row a bound of its k'-th
-    // neighbour distance; then the tiles that may hold a neighbour of some row of the block.
-    DevBuf<uint32_t> aptr, alist, aovf(c, n + 1);
+    // neighbour distance; then the tiles that may hold a neighbour of some row of the block. The second
+    // pass continues from the first's compacted buffers and thresholds over the remaining tiles (rows that
+    // overflowed in the first pass are already on the exact fallback list).
     st.tiles_bound = probe_lists(PRUNE_PROBE, aptr, alist);
-    PM_CUDA(cudaMemsetAsync(aovf.get() + n, 0, sizeof(uint32_t), c.stream));
-    run_filter(aptr.get(), alist.get(), aovf.get(), aovf.get() + n);
+    run_filter(aptr.get(), alist.get(), ovf.get(), ovf.get() + n, nullptr);
     c.check_errors("tensor-core kNN bound pass");
     DevBuf<float> ub(c, n_pad);
-    compact(ub.get());
+    resume.alloc(c, n_pad);
+    compact(ub.get(), resume.get());
     PruneInputs in;
     in.perm = perm.get();
     in.cell = cell.get();
@@ -1166,12 +1188,12 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     in.inv_s = 1.0f / s;
     in.blk0 = blk0;
     in.blk1 = blk1;
+    in.skip_ptr = aptr.get();
+    in.skip_list = alist.get();
     st.tiles_visited = build_pruned_tile_lists(c, in, tile_ptr, tile_list);
   }
   PM_CUDA(cudaEventRecord(ev[1], c.stream));
-  PM_CUDA(cudaMemsetAsync(ovf.get() + n, 0, sizeof(uint32_t), c.stream));
-  PM_CUDA(cudaMemsetAsync(fbk.get() + n, 0, sizeof(uint32_t), c.stream));
-  run_filter(tile_ptr.get(), tile_list.get(), ovf.get(), ovf.get() + n);
+  run_filter(tile_ptr.get(), tile_list.get(), ovf.get(), ovf.get() + n, prune ? resume.get() : nullptr);
   PM_CUDA(cudaEventRecord(ev[2], c.stream));
   c.check_errors("tensor-core kNN filter");
   float fms = 0.0f, bms = 0.0f;
@@ -1181,7 +1203,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   st.filter_ms = fms;
   st.bound_ms = bms;
 
-  compact(nullptr);
+  compact(nullptr, nullptr);
   const int di = static_cast<int>(d), ki = static_cast<int>(kp);
   auto rerank = [&](auto kern, int warps) {
     const unsigned rgrid = std::min<unsigned>(ceil_div(n, warps), c.sm_count * 32);
