@@ -369,10 +369,12 @@ __global__ void __launch_bounds__(PIV) pivot_near_kernel(const float* __restrict
 }
 
 // Per row block: the column tiles of its own cells, then those of the probe - 1 cells nearest each of its
-// own cells (ascending tile order in each group, no repeats). Count pass (list == nullptr) or fill pass.
+// own cells that holds fewer than min_cell points (ascending tile order in each group, no repeats). Count
+// pass (list == nullptr) or fill pass.
 constexpr int PL_MAX_WORDS = 4096;  // tile bitmask words in shared memory (ntiles <= 131,072)
 __global__ void __launch_bounds__(PIV) probe_lists_kernel(const uint32_t* __restrict__ cstart, uint64_t n, int ntiles,
-                                                          const uint32_t* __restrict__ near, int probe, int blk0,
+                                                          const uint32_t* __restrict__ near, int probe,
+                                                          uint32_t min_cell, int blk0,
                                                           const uint32_t* __restrict__ ptr,
                                                           uint32_t* __restrict__ counts, uint32_t* __restrict__ list) {
   __shared__ uint32_t own[PL_MAX_WORDS], other[PL_MAX_WORDS];
@@ -391,7 +393,7 @@ __global__ void __launch_bounds__(PIV) probe_lists_kernel(const uint32_t* __rest
   const bool mine = r0 < r1 && a < r1 && e > r0;
   if (mine) mark(own, p);
   __syncthreads();
-  if (mine)
+  if (mine && e - a < min_cell)
     for (int r = 1; r < probe; ++r) mark(other, static_cast<int>(near[p * probe + r]));
   __syncthreads();
   uint32_t c = 0;
@@ -423,8 +425,8 @@ __global__ void __launch_bounds__(PIV) probe_lists_kernel(const uint32_t* __rest
 }  // namespace
 
 uint64_t build_probe_tile_lists(Ctx& c, const float* d_x, uint64_t d, const uint32_t* d_piv_rows,
-                                const uint32_t* d_cstart, uint64_t n, uint64_t n_pad, int probe, uint64_t blk0,
-                                uint64_t blk1, DevBuf<uint32_t>& ptr, DevBuf<uint32_t>& list) {
+                                const uint32_t* d_cstart, uint64_t n, uint64_t n_pad, int probe, uint32_t min_cell,
+                                uint64_t blk0, uint64_t blk1, DevBuf<uint32_t>& ptr, DevBuf<uint32_t>& list) {
   const uint64_t nb = n_pad / TC_BM, ntiles = n_pad / TC_BN;
   PM_REQUIRE((ntiles + 31) / 32 <= static_cast<uint64_t>(PL_MAX_WORDS) && probe >= 1 && probe <= PIV,
              PACMAP_ERR_UNSUPPORTED, "probe lists: too many tiles");
@@ -434,7 +436,7 @@ uint64_t build_probe_tile_lists(Ctx& c, const float* d_x, uint64_t d, const uint
   PM_CUDA(cudaMemsetAsync(counts.get(), 0, nb * sizeof(uint32_t), c.stream));
   const unsigned nblk = static_cast<unsigned>(blk1 - blk0);
   if (nblk) {
-    probe_lists_kernel<<<nblk, PIV, 0, c.stream>>>(d_cstart, n, static_cast<int>(ntiles), near.get(), probe,
+    probe_lists_kernel<<<nblk, PIV, 0, c.stream>>>(d_cstart, n, static_cast<int>(ntiles), near.get(), probe, min_cell,
                                                    static_cast<int>(blk0), nullptr, counts.get(), nullptr);
     PM_LAUNCHED();
   }
@@ -446,7 +448,7 @@ uint64_t build_probe_tile_lists(Ctx& c, const float* d_x, uint64_t d, const uint
   PM_CUDA(cudaStreamSynchronize(c.stream));
   list.alloc(c, std::max<uint64_t>(total, 1));
   if (nblk) {
-    probe_lists_kernel<<<nblk, PIV, 0, c.stream>>>(d_cstart, n, static_cast<int>(ntiles), near.get(), probe,
+    probe_lists_kernel<<<nblk, PIV, 0, c.stream>>>(d_cstart, n, static_cast<int>(ntiles), near.get(), probe, min_cell,
                                                    static_cast<int>(blk0), ptr.get(), counts.get(), list.get());
     PM_LAUNCHED();
   }

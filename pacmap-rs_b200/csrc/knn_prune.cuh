@@ -31,12 +31,13 @@ struct PruneInputs {
 };
 
 // Per row block in [blk0, blk1): the column tiles of its own pivot cells, then those of the probe - 1
-// cells nearest each own cell (pivot-to-pivot distance), as a CSR list (ptr: n_pad / 256 + 1 offsets, list);
-// d_cstart: the PIV cell starts of the locality order. Returns the number of (block, tile) pairs. Needs
-// n_pad / 128 <= 131,072 column tiles.
+// cells nearest each own cell (pivot-to-pivot distance) that holds fewer than min_cell points (all of them
+// for min_cell = UINT32_MAX), as a CSR list (ptr: n_pad / 256 + 1 offsets, list); d_cstart: the PIV cell
+// starts of the locality order. Returns the number of (block, tile) pairs. Needs n_pad / 128 <= 131,072
+// column tiles.
 uint64_t build_probe_tile_lists(Ctx& c, const float* d_x, uint64_t d, const uint32_t* d_piv_rows,
-                                const uint32_t* d_cstart, uint64_t n, uint64_t n_pad, int probe, uint64_t blk0,
-                                uint64_t blk1, DevBuf<uint32_t>& ptr, DevBuf<uint32_t>& list);
+                                const uint32_t* d_cstart, uint64_t n, uint64_t n_pad, int probe, uint32_t min_cell,
+                                uint64_t blk0, uint64_t blk1, DevBuf<uint32_t>& ptr, DevBuf<uint32_t>& list);
 
 // Per row block in [blk0, blk1): the column tiles that may hold one of its rows' k' nearest points and are
 // not in its skip list, in the filter's sweep order, as a CSR list (ptr: n_pad / 256 + 1 offsets, list).

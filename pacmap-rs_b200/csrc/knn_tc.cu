@@ -71,7 +71,7 @@ struct alignas(8) TcShared {
 // The column-term tile rides with the first stage of each column tile.
 enum FilterMode { MODE_TILE = 0, MODE_KBLOCK = 1, MODE_STREAM = 2 };
 constexpr uint64_t PRUNE_MIN_ROWS = 32768;  // tile pruning from 256 column tiles on
-constexpr int PRUNE_PROBE = 2;              // cells per row block in the pruning's bound pass (own + nearest)
+constexpr int PRUNE_PROBE = 2;              // the bound pass: own cells (+ the nearest cell of a small one)
 constexpr int TC_SMEM_LIMIT = 232448;  // 227 KB of dynamic shared memory per block
 template <int KB, int MODE>
 struct FilterLayout {
@@ -859,41 +859,74 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
 #pragma unroll
     for (int ch = 0; ch < NC; ++ch) ra[ch] = ch < nc ? a[8 * ch + l8] : 0.0f;
     int nk = 0;
-    for (int e0 = 0; e0 < m; e0 += 4) {
-      const int e = e0 + grp;
-      const uint32_t jp = (e < m) ? cand[rb + e].x : static_cast<uint32_t>(r);
-      const uint32_t j = perm[jp];
-      const float* b = x + static_cast<uint64_t>(jp) * d;
-      float accl = 0.0f;
-      if (NC > 0) {
+    // 32 candidates per chunk: their indices and original ids by one coalesced and one parallel load, then
+    // two candidates per 8-lane group and pass, both rows' loads issued before either sum
+    for (int c0 = 0; c0 < m; c0 += 32) {
+      const bool mine = c0 + lane < m;
+      const uint32_t my_jp = mine ? cand[rb + c0 + lane].x : static_cast<uint32_t>(r);
+      const uint32_t my_j = perm[my_jp];
+      const int span = min(32, m - c0);
+      for (int q0 = 0; q0 < span; q0 += 8) {
+        float t2[2];
+        uint32_t jp2[2], j2[2];
+        bool real2[2];
 #pragma unroll
-        for (int ch = 0; ch < NC; ++ch) {
-          if (ch < nc) {
-            const float df = __fsub_rn(ra[ch], b[8 * ch + l8]);
-            accl = __fadd_rn(accl, __fmul_rn(df, df));
+        for (int h = 0; h < 2; ++h) {
+          const int q = q0 + 4 * h + grp;  // 0..31 within the chunk
+          jp2[h] = __shfl_sync(0xFFFFFFFFu, my_jp, q & 31);
+          j2[h] = __shfl_sync(0xFFFFFFFFu, my_j, q & 31);
+          real2[h] = (q < span) && (jp2[h] != r);
+        }
+        const float* b0 = x + static_cast<uint64_t>(jp2[0]) * d;
+        const float* b1 = x + static_cast<uint64_t>(jp2[1]) * d;
+        float acc0 = 0.0f, acc1 = 0.0f;
+        if (NC > 0) {
+          float v0[NC > 0 ? NC : 1], v1[NC > 0 ? NC : 1];
+#pragma unroll
+          for (int ch = 0; ch < NC; ++ch) {
+            v0[ch] = ch < nc ? b0[8 * ch + l8] : 0.0f;
+            v1[ch] = ch < nc ? b1[8 * ch + l8] : 0.0f;
+          }
+#pragma unroll
+          for (int ch = 0; ch < NC; ++ch) {
+            if (ch < nc) {
+              const float d0 = __fsub_rn(ra[ch], v0[ch]), d1 = __fsub_rn(ra[ch], v1[ch]);
+              acc0 = __fadd_rn(acc0, __fmul_rn(d0, d0));
+              acc1 = __fadd_rn(acc1, __fmul_rn(d1, d1));
+            }
+          }
+        } else {
+          for (int ch = 0; ch < nc; ++ch) {
+            const float av = a[8 * ch + l8];
+            const float d0 = __fsub_rn(av, b0[8 * ch + l8]), d1 = __fsub_rn(av, b1[8 * ch + l8]);
+            acc0 = __fadd_rn(acc0, __fmul_rn(d0, d0));
+            acc1 = __fadd_rn(acc1, __fmul_rn(d1, d1));
           }
         }
-      } else {
-        for (int ch = 0; ch < nc; ++ch) {
-          const float df = __fsub_rn(a[8 * ch + l8], b[8 * ch + l8]);
-          accl = __fadd_rn(accl, __fmul_rn(df, df));
+        t2[0] = 0.0f;
+        t2[1] = 0.0f;
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+          t2[0] = __fadd_rn(t2[0], __shfl_sync(0xFFFFFFFFu, acc0, (lane & ~7) + l));
+          t2[1] = __fadd_rn(t2[1], __shfl_sync(0xFFFFFFFFu, acc1, (lane & ~7) + l));
+        }
+        for (int q = nc * 8; q < d; ++q) {
+          const float av = a[q];
+          const float d0 = __fsub_rn(av, b0[q]), d1 = __fsub_rn(av, b1[q]);
+          t2[0] = __fadd_rn(t2[0], __fmul_rn(d0, d0));
+          t2[1] = __fadd_rn(t2[1], __fmul_rn(d1, d1));
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float dist = __fsqrt_rn(t2[h]);
+          const unsigned bal = __ballot_sync(0xFFFFFFFFu, real2[h] && l8 == 0);
+          if (real2[h] && l8 == 0) {
+            const int pos = nk + __popc(bal & ((1u << lane) - 1u));
+            keys[pos] = (static_cast<uint64_t>(total_key(dist)) << 32) | j2[h];
+          }
+          nk += __popc(bal);
         }
       }
-      float t = 0.0f;
-#pragma unroll
-      for (int l = 0; l < 8; ++l) t = __fadd_rn(t, __shfl_sync(0xFFFFFFFFu, accl, (lane & ~7) + l));
-      for (int q = nc * 8; q < d; ++q) {
-        const float df = __fsub_rn(a[q], b[q]);
-        t = __fadd_rn(t, __fmul_rn(df, df));
-      }
-      const float dist = __fsqrt_rn(t);
-      const bool real = (e < m) && (jp != r);
-      const unsigned bal = __ballot_sync(0xFFFFFFFFu, real && l8 == 0);
-      if (real && l8 == 0) {
-        const int pos = nk + __popc(bal & ((1u << lane) - 1u));
-        keys[pos] = (static_cast<uint64_t>(total_key(dist)) << 32) | j;
-      }
-      nk += __popc(bal);
     }
     __syncwarp();
     if (nk < K) {  // fewer certified candidates than neighbours (non-finite data): exact fallback
@@ -988,10 +1021,11 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   // contiguous ranges of the locality order: cell p starts at the first chunk's offset for p.
   const uint64_t blocks_all = nblocks;
   const uint64_t sblk0 = blocks_all * shard.index / shard.count, sblk1 = blocks_all * (shard.index + 1) / shard.count;
-  auto probe_lists = [&](int probe, DevBuf<uint32_t>& tile_ptr, DevBuf<uint32_t>& tile_list) -> uint64_t {
+  auto probe_lists = [&](int probe, uint32_t min_cell, DevBuf<uint32_t>& tile_ptr,
+                         DevBuf<uint32_t>& tile_list) -> uint64_t {
     if (ntl <= 131072)  // on the device: the cell starts are the first chunk's offsets
-      return build_probe_tile_lists(c, d_x, d, piv_rows.get(), cell_counts.get(), n, n_pad, probe, sblk0, sblk1,
-                                    tile_ptr, tile_list);
+      return build_probe_tile_lists(c, d_x, d, piv_rows.get(), cell_counts.get(), n, n_pad, probe, min_cell, sblk0,
+                                    sblk1, tile_ptr, tile_list);
     std::vector<uint32_t> cstart(PIV + 1);
     DevBuf<float> piv(c, static_cast<uint64_t>(PIV) * d);
     gather_pivots_kernel<<<PIV, 128, 0, c.stream>>>(d_x, piv_rows.get(), static_cast<int>(d), piv.get());
@@ -1044,7 +1078,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   };
 
   DevBuf<uint32_t> tile_ptr, tile_list;
-  if (nprobe > 0 && nprobe < PIV) probe_lists(nprobe, tile_ptr, tile_list);
+  if (nprobe > 0 && nprobe < PIV) probe_lists(nprobe, 0xFFFFFFFFu, tile_ptr, tile_list);
 
   DevBuf<uint16_t> H(c, n_pad * KP);
   DevBuf<float> xperm(c, n * d);
@@ -1169,7 +1203,8 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     // neighbour distance; then the tiles that may hold a neighbour of some row of the block. The second
     // pass continues from the first's compacted buffers and thresholds over the remaining tiles (rows that
     // overflowed in the first pass are already on the exact fallback list).
-    st.tiles_bound = probe_lists(PRUNE_PROBE, aptr, alist);
+    // a cell of at least 4 (k'+1) points bounds its rows by itself; smaller cells add their nearest cell
+    st.tiles_bound = probe_lists(PRUNE_PROBE, static_cast<uint32_t>(4 * rank), aptr, alist);
     run_filter(aptr.get(), alist.get(), ovf.get(), ovf.get() + n, nullptr);
     c.check_errors("tensor-core kNN bound pass");
     DevBuf<float> ub(c, n_pad);
