@@ -15,6 +15,8 @@
 // compare per register and a vote; the MN variant also keeps row i of x in registers. The general
 // variants (every lane replays the stream, lists read from memory) serve the shapes beyond those
 // registers. Both variants consume the same words in the same order: the pairs are identical.
+#include <cuda_fp16.h>
+
 #include "engine.cuh"
 
 namespace pacmap {
@@ -506,6 +508,220 @@ __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_spec_kernel(const flo
   }
 }
 
+// The screened variant of sample_mn_spec_kernel (d a multiple of 16, at most 256): the candidates' rows
+// are read from an fp16 copy h of x (half the bytes) with eps_j = |x_j - h_j| (rounded up) per row. By the
+// triangle inequality the true distance lies within dist(x_i, h_j) -/+ eps_j, and the reference's f32
+// distance within a further 2^-15 relative (its f32 sum over <= 256 terms, and this kernel's own). When
+// those intervals settle both which two candidates are the closest and their order, the slot's pick is
+// the reference's pick; otherwise the slot's six distances are computed exactly as distance.rs:50-75
+// does. Exact ties always overlap, so they are always settled by the exact distances and the draw order.
+constexpr float MN_REL = 3.0517578125e-05f;  // 2^-15
+template <int E>  // elements per lane of the screening (d = 8 E)
+__global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_screen_kernel(
+    const float* __restrict__ x, const __half* __restrict__ h, const float* __restrict__ eps, uint64_t n, int d,
+    uint32_t n_mn, uint64_t seed, uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_cand[MS_WARPS][MS_MAXC];
+  __shared__ float s_lo[MS_WARPS][MS_MAXC], s_hi[MS_WARPS][MS_MAXC];
+  const int warp = threadIdx.x >> 5;
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * MS_WARPS;
+  const uint32_t lane = lane_id();
+  const int l8 = lane & 7;
+  const unsigned gbase = lane & ~7u;
+  const int grp = lane >> 3;
+  const int nc = d >> 3;
+  const int total = static_cast<int>(n_mn) * 6;
+  uint32_t* cs = s_cand[warp];
+  float* lo_s = s_lo[warp];
+  float* hi_s = s_hi[warp];
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * MS_WARPS + warp; i < n; i += warps) {
+    // 1. every slot's draws (self and repeats within the slot rejected, as in the rule)
+    WarpStream s(seed, i);
+    uint64_t budget = SAMPLE_ATTEMPT_CAP;
+    bool failed = false;
+    for (uint32_t jslot = 0; jslot < n_mn && !failed; ++jslot) {
+      uint32_t cand[6] = {0, 0, 0, 0, 0, 0};
+      uint32_t cnt = 0;
+      while (cnt < 6) {
+        uint32_t j;
+        if (!s.uniform(static_cast<uint32_t>(n), j, budget)) {
+          failed = true;
+          break;
+        }
+        if (j == i) continue;
+        bool dup = false;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) dup |= (t < static_cast<int>(cnt) && cand[t] == j);
+        if (dup) continue;
+#pragma unroll
+        for (int t = 0; t < 6; ++t)
+          if (t == static_cast<int>(cnt)) cand[t] = j;
+        ++cnt;
+      }
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (static_cast<int>(lane) == t) cs[jslot * 6 + t] = cand[t];
+    }
+    __syncwarp();
+    if (failed) {  // the sequential rule reports the failure
+      mn_point_sequential(x, n, d, n_mn, seed, i, out, err);
+      continue;
+    }
+    // 2. screening distances on the fp16 rows: lane l8 of a group holds E consecutive elements
+    const float* a = x + i * d;
+    float xe[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) xe[q] = a[l8 * E + q];
+    for (int c0 = 0; c0 < total; c0 += 8) {
+      const int ca = c0 + grp, cb = c0 + 4 + grp;
+      const uint32_t ja = ca < total ? cs[ca] : static_cast<uint32_t>(i);
+      const uint32_t jb = cb < total ? cs[cb] : static_cast<uint32_t>(i);
+      const uint4* pa = reinterpret_cast<const uint4*>(h + static_cast<uint64_t>(ja) * d + l8 * E);
+      const uint4* pb = reinterpret_cast<const uint4*>(h + static_cast<uint64_t>(jb) * d + l8 * E);
+      uint4 va[E / 8], vb[E / 8];
+#pragma unroll
+      for (int q = 0; q < E / 8; ++q) {
+        va[q] = pa[q];
+        vb[q] = pb[q];
+      }
+      const float ea = eps[ja], eb = eps[jb];
+      float sa = 0.0f, sb = 0.0f;
+#pragma unroll
+      for (int q = 0; q < E / 8; ++q) {
+        const __half2* ha = reinterpret_cast<const __half2*>(&va[q]);
+        const __half2* hb = reinterpret_cast<const __half2*>(&vb[q]);
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const float2 fa = __half22float2(ha[w]), fb = __half22float2(hb[w]);
+          const float a0 = xe[8 * q + 2 * w] - fa.x, a1 = xe[8 * q + 2 * w + 1] - fa.y;
+          const float b0 = xe[8 * q + 2 * w] - fb.x, b1 = xe[8 * q + 2 * w + 1] - fb.y;
+          sa = fmaf(a0, a0, fmaf(a1, a1, sa));
+          sb = fmaf(b0, b0, fmaf(b1, b1, sb));
+        }
+      }
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) {
+        sa += __shfl_xor_sync(0xFFFFFFFFu, sa, o);
+        sb += __shfl_xor_sync(0xFFFFFFFFu, sb, o);
+      }
+      if (l8 == 0) {
+        const float da = sqrtf(sa), db = sqrtf(sb);
+        // |ref - true| <= (d/8 + 12) 2^-24 true and |da - |x_i - h_j|| <= (d + 4) 2^-25 da: 2^-15 covers both
+        if (ca < total) {
+          lo_s[ca] = da * (1.0f - MN_REL) - ea * (1.0f + MN_REL);
+          hi_s[ca] = (da + ea) * (1.0f + MN_REL);
+        }
+        if (cb < total) {
+          lo_s[cb] = db * (1.0f - MN_REL) - eb * (1.0f + MN_REL);
+          hi_s[cb] = (db + eb) * (1.0f + MN_REL);
+        }
+      }
+    }
+    __syncwarp();
+    // 3. lane j: slot j settled by the intervals? the two lowest upper bounds must lie below every other
+    //    lower bound, and the lower of the two below the other's lower bound
+    uint32_t pick = 0;
+    bool exact = false;
+    if (lane < n_mn) {
+      float hi1 = 3.4e38f, hi2 = 3.4e38f;
+      int t1 = 0, t2 = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const float hv = hi_s[lane * 6 + t];
+        if (hv < hi1) {
+          hi2 = hi1;
+          t2 = t1;
+          hi1 = hv;
+          t1 = t;
+        } else if (hv < hi2) {
+          hi2 = hv;
+          t2 = t;
+        }
+      }
+      bool sure = hi1 < lo_s[lane * 6 + t2] && t1 != t2;
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        if (t != t1 && t != t2) sure = sure && hi2 < lo_s[lane * 6 + t];
+      exact = !sure;
+      pick = cs[lane * 6 + t2];
+    }
+    // 4. unsettled slots: the reference's exact distances of their six candidates (group g: slots t = g, g + 4)
+    unsigned need = __ballot_sync(0xFFFFFFFFu, exact);
+    while (need) {
+      const int js = __ffs(need) - 1;
+      need &= need - 1;
+      float dist[6];
+#pragma unroll
+      for (int pass = 0; pass < 2; ++pass) {
+        const int t = pass * 4 + grp;
+        const bool active = t < 6;
+        const uint32_t cj = active ? cs[js * 6 + t] : static_cast<uint32_t>(i);
+        const float r = group8_ref_dist(a, x + static_cast<uint64_t>(cj) * d, d, l8, gbase);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const float v = __shfl_sync(0xFFFFFFFFu, r, g * 8);
+          if (pass * 4 + g < 6) dist[pass * 4 + g] = v;
+        }
+      }
+      uint64_t best0 = ~0ull, best1 = ~0ull;
+      uint32_t id1 = 0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const uint64_t key = (static_cast<uint64_t>(total_key(dist[t])) << 3) | static_cast<uint64_t>(t);
+        if (key < best0) {
+          best1 = best0;
+          best0 = key;
+        } else if (key < best1) {
+          best1 = key;
+        }
+      }
+      id1 = cs[js * 6 + static_cast<int>(best1 & 7u)];
+      if (static_cast<int>(lane) == js) pick = id1;
+    }
+    (void)nc;
+    // 5. the draws were made without the earlier picks: valid iff no candidate of slot j is a pick of a
+    //    slot before j; otherwise the sequential rule redoes the point
+    bool clash = false;
+    for (uint32_t q = 0; q + 1 < n_mn; ++q) {
+      const uint32_t pq = __shfl_sync(0xFFFFFFFFu, pick, q);
+      if (lane < n_mn && q < lane) {
+#pragma unroll
+        for (int t = 0; t < 6; ++t) clash |= cs[lane * 6 + t] == pq;
+      }
+    }
+    __syncwarp();
+    if (__any_sync(0xFFFFFFFFu, clash)) {
+      mn_point_sequential(x, n, d, n_mn, seed, i, out, err);
+      continue;
+    }
+    if (lane < n_mn) {
+      out[(i * n_mn + lane) * 2 + 0] = static_cast<uint32_t>(i);
+      out[(i * n_mn + lane) * 2 + 1] = pick;
+    }
+    __syncwarp();
+  }
+}
+
+// fp16 copy of x and each row's rounding-residual norm |x_j - h_j| (rounded up), one warp per row.
+__global__ void half_rows_kernel(const float* __restrict__ x, uint64_t n, int d, __half* __restrict__ h,
+                                 float* __restrict__ eps) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += warps) {
+    float ss = 0.0f;
+    for (int c = lane; c < d; c += 32) {
+      const float v = x[r * d + c];
+      const __half hv = __float2half_rn(v);
+      h[r * d + c] = hv;
+      const float res = v - __half2float(hv);  // exact (Sterbenz: hv is within a factor 2 of v, or both tiny)
+      ss = fmaf(res, res, ss);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xFFFFFFFFu, ss, o);
+    // the f32 sum of d squares is within d 2^-24 relative, its square root within half that: 2^-15 covers both
+    if (lane == 0) eps[r] = sqrtf(ss) * (1.0f + MN_REL) + 1e-30f;
+  }
+}
+
 // sample_mn_kernel with the picks (n_mn <= 32) in one register per lane and row i of x (d <= 8 NC)
 // in NC registers of each 8-lane group.
 template <int NC>
@@ -677,6 +893,22 @@ void sample_mn_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, uint64_
   const int di = static_cast<int>(d);
   const uint32_t m32 = static_cast<uint32_t>(n_mn);
   const bool spec = n_mn <= 32 && n >= n_mn + 7;
+  if (spec && (d == 128 || d == 256)) {
+    // screened on an fp16 copy (half the gathered bytes); the unsettled slots use the exact rows
+    DevBuf<__half> h(c, n * d);
+    DevBuf<float> eps(c, n);
+    half_rows_kernel<<<static_cast<unsigned>(std::min<uint64_t>(ceil_div(n, 8), c.sm_count * 32ull)), 256, 0,
+                       c.stream>>>(d_xp, n, di, h.get(), eps.get());
+    PM_LAUNCHED();
+    if (d == 128)
+      sample_mn_screen_kernel<16><<<grid, MS_WARPS * 32, 0, c.stream>>>(d_xp, h.get(), eps.get(), n, di, m32, seed,
+                                                                         d_pmn, c.d_err);
+    else
+      sample_mn_screen_kernel<32><<<grid, MS_WARPS * 32, 0, c.stream>>>(d_xp, h.get(), eps.get(), n, di, m32, seed,
+                                                                         d_pmn, c.d_err);
+    PM_LAUNCHED();
+    return;
+  }
   if (spec && d <= 128)
     sample_mn_spec_kernel<16><<<grid, MS_WARPS * 32, 0, c.stream>>>(d_xp, n, di, m32, seed, d_pmn, c.d_err);
   else if (spec && d <= 256)

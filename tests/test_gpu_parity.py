@@ -97,7 +97,9 @@ def test_reselect_bit_exact(lib, orc):
 # ----------------------------------------------------------------------------------------------------
 # Philox samplers (sampling.rs:37-142): bit-exact against the oracle's host mirror.
 # ----------------------------------------------------------------------------------------------------
-@pytest.mark.parametrize("n,d,k,n_mn,n_fp", [(3000, 50, 10, 5, 20), (500, 8, 40, 20, 80), (12, 3, 10, 5, 20)])
+@pytest.mark.parametrize("n,d,k,n_mn,n_fp", [(3000, 50, 10, 5, 20), (500, 8, 40, 20, 80), (12, 3, 10, 5, 20),
+                                             # the fp16-screened mid-near path (d = 128, 256)
+                                             (3000, 128, 10, 5, 20), (2000, 256, 12, 6, 24), (20, 128, 5, 10, 5)])
 def test_samplers_bit_exact(lib, orc, n, d, k, n_mn, n_fp):
     x = _mixture(n, d, seed=5)
     xp, *_ = orc.preprocess(x)
@@ -108,6 +110,19 @@ def test_samplers_bit_exact(lib, orc, n, d, k, n_mn, n_fp):
         pmn, pfp = lib.stages.sample_pairs(xp, pnn, kk, n_mn, n_fp, seed)
         assert np.array_equal(pfp, orc.sample_fp_pairs(pnn, n, kk, n_fp, seed))
         assert np.array_equal(pmn, orc.sample_mn_pairs(xp, n_mn, seed))
+
+
+def test_mn_screening_ties_and_duplicates_bit_exact(lib, orc):
+    # many exact duplicates and quantised values: the fp16 intervals overlap on ties, so those slots take the
+    # exact distances and the draw order, as the rule does
+    x = np.round(_mixture(4000, 128, seed=6) * 2.0) / 2.0
+    x[100:400] = x[7]
+    x[1000:1050] = x[8]
+    xp, *_ = orc.preprocess(x.astype(np.float32))
+    pnn = np.zeros((4000 * 10, 2), np.uint32)
+    for seed in (3, 77):
+        pmn, _ = lib.stages.sample_pairs(xp, pnn, 10, 20, 0, seed)
+        assert np.array_equal(pmn, orc.sample_mn_pairs(xp, 20, seed))
 
 
 def test_generate_pairs_bit_exact(lib, orc):
