@@ -13,10 +13,11 @@
 //     Cauchy-Schwarz bound of h.l + l.h + l.l, eta = tensor-core accumulation, gamma = every f32
 //     rounding incl. the reference's own distance sum), the reference's squared distance lies in
 //     [LB, UB] = [v + n_i - 2e_i, v + 4e_j + n_i + 2e_i].
-//     Each row keeps a buffer of candidates with v <= theta_i, where theta_i comes from the (k'+1)-th
-//     smallest UB seen so far (the +1 covers the row itself); when the buffer fills, the owning warp
-//     compacts it (the rank-th smallest upper bound by bisection on warp-wide counts). Any true
-//     neighbour has LB <= k'-th UB, so it is never dropped.
+//     Each row keeps a buffer of candidates (j, u = v + 4 e_j) with v <= theta_i, where theta_i comes from
+//     the (k'+1)-th smallest UB seen so far (the +1 covers the row itself); when the buffer fills, the
+//     owning warp compacts it (the rank-th smallest u by bisection on warp-wide counts; inside the filter
+//     the kept set is u <= theta + max 4 e, a superset of the band, so no per-entry gather is needed).
+//     Any true neighbour has LB <= k'-th UB, so it is never dropped.
 //  3. knn_rerank_kernel: the final threshold, then the reference's exact f32 distance of every
 //     survivor, sorted by (distance, index): the rows of knn.rs.
 //  Rows whose candidate band does not fit the buffer (e.g. thousands of exact duplicates) are
@@ -100,57 +101,81 @@ __device__ __forceinline__ float theta_from(uint32_t ukey, float n_i, float e4_i
   return base + slack;
 }
 
-// Register-resident compaction of one row's buffer (m <= 32 * PER (index, v) entries), one warp: the
-// entries are loaded once with their upper bounds u = v + 4 e_j, the rank-`rank` smallest u is found
-// by bisection on the registers, entries with v <= theta survive (order kept) and are written back once.
+// Candidate entries are (index j, u = v + 4 e_j): u is the upper bound of the reference's squared distance
+// less n_i + 2 e_i, v = u - 4 e_j the lower one less n_i - 2 e_i (both scaled by s^2).
+//
+// A row's buffer in registers (m <= 32 * PER entries), loaded once per compaction by the whole warp.
 template <int PER>
-__device__ __forceinline__ int warp_compact_regs(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
-                                                 const float2* __restrict__ ge, float& theta_out,
-                                                 uint32_t* ukey_out = nullptr) {
-  const int lane = threadIdx.x & 31;
+struct RowRegs {
   uint32_t ri[PER];
-  float rv[PER];
-  uint32_t rk[PER];
+  float ru[PER];
+};
+template <int PER>
+__device__ __forceinline__ void load_row(const uint2* __restrict__ cand, int m, RowRegs<PER>& r) {
+  const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
     const int e = q * 32 + lane;
-    const bool in = e < m;
-    const uint2 cv = in ? cand[e] : make_uint2(0u, 0u);
-    ri[q] = cv.x;
-    rv[q] = __uint_as_float(cv.y);
-    // the candidate's upper bound u = v + 4 e_j (e_j of its column)
-    rk[q] = in ? total_key(rv[q] + __ldg(&ge[ri[q]].y)) : 0xFFFFFFFFu;
+    const uint2 cv = e < m ? cand[e] : make_uint2(0u, 0u);
+    r.ri[q] = cv.x;
+    r.ru[q] = __uint_as_float(cv.y);
   }
-  // The rank-th smallest key by bisection on [min key, max key] with warp-wide counts (no shared
-  // memory, no atomics): the smallest key value T with #{keys <= T} >= rank.
+}
+
+// Compaction of one row's buffer from its registers, one warp: the rank-`rank` smallest u by bisection
+// on warp-wide counts, theta from it, and the entries of the row's certified band (v <= theta) written
+// back in order. With ge (the separate compaction kernels) v = u - 4 e_j is recovered exactly up to one
+// rounding (kept when within 2^-22 of the magnitudes above theta); without it (inside the filter, where
+// a gather per entry would stall the epilogue) an entry is kept when u <= theta + e4max, a superset.
+template <int PER>
+__device__ __forceinline__ int compact_row(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
+                                           const RowRegs<PER>& r, float e4max, const float2* __restrict__ ge,
+                                           float& theta_out, uint32_t* ukey_out = nullptr) {
+  const int lane = threadIdx.x & 31;
+  uint32_t rk[PER];
   uint32_t kmin = 0xFFFFFFFFu, kmax = 0u;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
-    if (q * 32 + lane < m) {
+    const bool in = q * 32 + lane < m;
+    rk[q] = in ? total_key(r.ru[q]) : 0xFFFFFFFFu;
+    if (in) {
       kmin = min(kmin, rk[q]);
       kmax = max(kmax, rk[q]);
     }
   }
+  // The rank-th smallest key by bisection on [min key, max key] with warp-wide counts (no shared
+  // memory, no atomics): the smallest key value T with #{keys <= T} >= rank.
   uint32_t lo = __reduce_min_sync(0xFFFFFFFFu, kmin), hi = __reduce_max_sync(0xFFFFFFFFu, kmax);
   while (lo < hi) {
     const uint32_t mid = lo + ((hi - lo) >> 1);
     uint32_t cnt = 0;
 #pragma unroll
-    for (int q = 0; q < PER; ++q) cnt += (q * 32 + lane < m && rk[q] <= mid) ? 1u : 0u;
+    for (int q = 0; q < PER; ++q) cnt += (rk[q] <= mid) ? 1u : 0u;
     cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
     if (cnt >= static_cast<uint32_t>(rank)) hi = mid;
     else lo = mid + 1u;
   }
   const uint32_t prefix = lo;
   const float th = theta_from(prefix, n_i, e4_i);
+  float e4j[PER];
+  if (ge) {
+#pragma unroll
+    for (int q = 0; q < PER; ++q) e4j[q] = q * 32 + lane < m ? __ldg(&ge[r.ri[q]].y) : 0.0f;
+  }
   int out = 0;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
-    const bool keep = (q * 32 + lane < m) && rv[q] <= th;
+    bool keep = q * 32 + lane < m;
+    if (ge) {
+      const float v = r.ru[q] - e4j[q];
+      keep = keep && v <= th + 2.384185791015625e-07f * (fabsf(r.ru[q]) + e4j[q]);
+    } else {
+      keep = keep && r.ru[q] <= (th + e4max) + 2.384185791015625e-07f * (fabsf(th) + e4max);
+    }
     const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
     if (keep) {
       const int pos = out + __popc(bal & ((1u << lane) - 1u));
-      cand[pos] = make_uint2(ri[q], __float_as_uint(rv[q]));
+      cand[pos] = make_uint2(r.ri[q], __float_as_uint(r.ru[q]));
     }
     out += __popc(bal);
   }
@@ -451,7 +476,7 @@ __global__ void split_rows_kernel(const float* __restrict__ x, const uint32_t* _
 // operand sums them to -g_j / 2 whatever the swizzle order of the two 16-byte halves.
 __global__ void bound_kernel(uint64_t n, uint64_t n_pad, int d, int KP, float rho, const float* __restrict__ nrm,
                              const float* __restrict__ A, const float* __restrict__ B, float2* __restrict__ ge,
-                             uint16_t* __restrict__ gq) {
+                             uint16_t* __restrict__ gq, uint32_t* __restrict__ e4max_bits) {
   const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (j >= n_pad) return;
   uint16_t parts[3] = {0, 0, 0};
@@ -471,6 +496,7 @@ __global__ void bound_kernel(uint64_t n, uint64_t n_pad, int d, int KP, float rh
     const float e_safe = e * (1.0f + 9.765625e-04f);  // 2^-10 relative margin on the bound itself
     const float g = nrm[j] - 2.0f * e_safe;
     ge[j] = make_float2(g, 4.0f * e_safe);
+    atomicMax(e4max_bits, __float_as_uint(4.0f * e_safe));  // non-negative floats order as their bits
     const float q = -0.25f * g;
     const __nv_bfloat16 p0 = __float2bfloat16_rn(q);
     const float r1 = q - __bfloat162float(p0);
@@ -504,7 +530,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const uint32_t* __restrict__ perm, int rank, uint2* __restrict__ cand, int* __restrict__ cand_cnt,
     uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err,
     int block_offset, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_list,
-    const float* __restrict__ resume_theta) {
+    const float* __restrict__ resume_theta, const uint32_t* __restrict__ e4max_bits) {
   using L = FilterLayout<KB, MODE>;
   constexpr int NST = L::NST;
   constexpr int C = 32 * PER;
@@ -705,6 +731,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const float n_i = valid ? nrm[row] : 0.0f;
     const float e4_i = valid ? ge[row].y : 0.0f;
     const uint64_t cbase = row * static_cast<uint64_t>(C);
+    const float e4max = __uint_as_float(*e4max_bits);
     bool ok = true;
     auto screen = [&](const uint32_t (&r)[32], int colb) {
       float m8[4];
@@ -722,7 +749,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
             for (int c = 8 * g; c < 8 * g + 8; ++c) {
               const float v = -2.0f * __uint_as_float(r[c]);
               if (v <= theta) {
-                cand[cbase + cnt] = make_uint2(static_cast<uint32_t>(colb + c), __float_as_uint(v));
+                const uint32_t col = static_cast<uint32_t>(colb + c);
+                cand[cbase + cnt] = make_uint2(col, __float_as_uint(v + __ldg(&ge[col].y)));
                 ++cnt;
               }
             }
@@ -753,26 +781,41 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh->tmem_empty[acc]);
       // Compact full buffers so that the next tile (<= 128 insertions) always fits.
+      // The next row's entries are loaded before the current row is compacted (their latency overlaps).
       unsigned need = __ballot_sync(0xFFFFFFFFu, cnt > C - TC_BN);
-      while (need) {
-        const int L = __ffs(need) - 1;
+      if (need) {
+        int L = __ffs(need) - 1;
         need &= need - 1;
-        const uint64_t rb = __shfl_sync(0xFFFFFFFFu, cbase, L);
-        const int m = __shfl_sync(0xFFFFFFFFu, cnt, L);
-        const float nL = __shfl_sync(0xFFFFFFFFu, n_i, L);
-        const float eL = __shfl_sync(0xFFFFFFFFu, e4_i, L);
-        float th;
-        const int kept = warp_compact_regs<PER>(cand + rb, m, min(rank, m), nL, eL, ge, th);
-        if (lane == L) {
-          theta = th;
-          cnt = kept;
-          if (cnt > C - TC_BN) {  // the band does not fit: exact recomputation later
-            theta = -__int_as_float(0x7f800000);
-            cnt = 0;
-            overflow_rows[atomicAdd(n_overflow, 1u)] = perm[row];
+        RowRegs<PER> cur;
+        load_row<PER>(cand + __shfl_sync(0xFFFFFFFFu, cbase, L), __shfl_sync(0xFFFFFFFFu, cnt, L), cur);
+        while (true) {
+          // PER > 16 keeps one row in registers at a time (two would spill)
+          const int L2 = need ? __ffs(need) - 1 : -1;
+          RowRegs<PER> nxt;
+          if (PER <= 16 && L2 >= 0)
+            load_row<PER>(cand + __shfl_sync(0xFFFFFFFFu, cbase, L2), __shfl_sync(0xFFFFFFFFu, cnt, L2), nxt);
+          const uint64_t rb = __shfl_sync(0xFFFFFFFFu, cbase, L);
+          const int m = __shfl_sync(0xFFFFFFFFu, cnt, L);
+          const float nL = __shfl_sync(0xFFFFFFFFu, n_i, L);
+          const float eL = __shfl_sync(0xFFFFFFFFu, e4_i, L);
+          float th;
+          const int kept = compact_row<PER>(cand + rb, m, min(rank, m), nL, eL, cur, e4max, nullptr, th);
+          if (lane == L) {
+            theta = th;
+            cnt = kept;
+            if (cnt > C - TC_BN) {  // the band does not fit: exact recomputation later
+              theta = -__int_as_float(0x7f800000);
+              cnt = 0;
+              overflow_rows[atomicAdd(n_overflow, 1u)] = perm[row];
+            }
           }
+          __syncwarp();
+          if (L2 < 0) break;
+          need &= need - 1;
+          L = L2;
+          if (PER <= 16) cur = nxt;
+          else load_row<PER>(cand + __shfl_sync(0xFFFFFFFFu, cbase, L), __shfl_sync(0xFFFFFFFFu, cnt, L), cur);
         }
-        __syncwarp();
       }
     }
     if (!ok) {
@@ -818,7 +861,9 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     float th;
     uint32_t ukey = 0;
     const float n_i = nrm[r], e4_i = ge[r].y;
-    const int m = warp_compact_regs<PER>(cand + rb, m0, min(rank, m0), n_i, e4_i, ge, th, &ukey);
+    RowRegs<PER> regs;
+    load_row<PER>(cand + rb, m0, regs);
+    const int m = compact_row<PER>(cand + rb, m0, min(rank, m0), n_i, e4_i, regs, 0.0f, ge, th, &ukey);
     if (lane == 0) {
       cand_cnt[r] = m;
       if (theta_out) theta_out[r] = th;
@@ -1103,8 +1148,10 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     sb += hpart[2 * b + 1];
   }
   const float rho = (sa > 0.0 && sb > 0.0) ? static_cast<float>(std::sqrt(sb / sa)) : 1e-4f;
+  DevBuf<uint32_t> e4max(c, 1);
+  PM_CUDA(cudaMemsetAsync(e4max.get(), 0, sizeof(uint32_t), c.stream));
   bound_kernel<<<ceil_div(n_pad, 256), 256, 0, c.stream>>>(n, n_pad, static_cast<int>(d), KP, rho, nrm.get(), A.get(),
-                                                          B.get(), ge.get(), gq.get());
+                                                          B.get(), ge.get(), gq.get(), e4max.get());
   PM_LAUNCHED();
 
   CUtensorMap map;
@@ -1153,7 +1200,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
       if (grid == 0) return;
       kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, KB, idesc, ge.get(), nrm.get(), perm.get(), rank,
                                                  cand.get(), ccnt.get(), ovf_rows, n_ovf, c.d_err,
-                                                 static_cast<int>(blk0), lptr, llist, resume_theta);
+                                                 static_cast<int>(blk0), lptr, llist, resume_theta, e4max.get());
     };
     const bool p16 = PER == 16;
     if (mode == MODE_STREAM) {
