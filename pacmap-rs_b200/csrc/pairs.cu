@@ -566,6 +566,17 @@ __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_screen_kernel(
       mn_point_sequential(x, n, d, n_mn, seed, i, out, err);
       continue;
     }
+    // every candidate's fp16 row and bound towards L2 at once (the passes below then wait on L2, not on
+    // one DRAM round trip per pass)
+    {
+      const int lines = (d * 2 + 127) / 128;
+      for (int q = static_cast<int>(lane); q < total * lines; q += 32) {
+        const int c = q / lines, ln = q - c * lines;
+        const char* line = reinterpret_cast<const char*>(h + static_cast<uint64_t>(cs[c]) * d) + ln * 128;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+      }
+      for (int c = static_cast<int>(lane); c < total; c += 32) asm volatile("prefetch.global.L2 [%0];" ::"l"(eps + cs[c]));
+    }
     // 2. screening distances on the fp16 rows: lane l8 of a group holds E consecutive elements
     const float* a = x + i * d;
     float xe[E];
