@@ -3,7 +3,9 @@
 //
 // K7 build_csr: every pair (i, j), i != j, of the three lists becomes two entries -- partner j in the
 //    segment (i, type) and partner i in the segment (j, type) -- via a counting sort, then each segment
-//    is sorted by partner. A pair's contribution to each endpoint is bit-identical whichever endpoint
+//    is sorted by partner. When the lists are grouped by point (the generated ones are), a segment is
+//    point i's own partners in pair order followed by the points that drew i, sorted: only that second
+//    part is placed by atomics and sorted. A pair's contribution to each endpoint is bit-identical whichever endpoint
 //    lists it (the squared distance and the weight use |y_i - y_j| only), so the sorted segments fix
 //    one deterministic summation order with no floating-point atomics. (The reference's rayon reduce,
 //    gradient.rs:53-70, has no fixed order at all.)
@@ -51,6 +53,69 @@ __global__ void csr_fill_kernel(const uint32_t* __restrict__ pairs, uint64_t P, 
     col[atomicAdd(&cursor[static_cast<uint64_t>(a) * 3 + type], 1u)] = b;
     col[atomicAdd(&cursor[static_cast<uint64_t>(b) * 3 + type], 1u)] = a;
   }
+}
+
+// The generated pair lists hold each point's pairs together (rows i*k .. i*k + k - 1 start with i). Then
+// a segment's forward entries (partners of its own pairs) are written in pair order without atomics, and
+// only the reverse entries (points that drew it) are placed by atomics and sorted.
+__global__ void grouped_check_kernel(const uint32_t* __restrict__ pairs, uint64_t P, uint32_t k,
+                                     uint32_t* __restrict__ flag) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  bool ok = true;
+  for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += stride)
+    ok = ok && pairs[2 * p] == static_cast<uint32_t>(p / k);
+  if (!__all_sync(0xFFFFFFFFu, ok) && (threadIdx.x & 31) == 0) *flag = 0u;
+}
+
+// Forward counts of grouped lists: segment (i, type) gets the partners j != i of point i's k pairs.
+__global__ void csr_fwd_count_kernel(const uint32_t* __restrict__ pairs, uint64_t n, uint32_t k, int type,
+                                     uint32_t* __restrict__ fwd, uint32_t* __restrict__ cnt,
+                                     uint32_t* __restrict__ err) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t c = 0;
+  for (uint32_t q = 0; q < k; ++q) {
+    const uint32_t j = pairs[2 * (i * k + q) + 1];
+    if (j >= n) atomicOr(err, DEV_ERR_PAIR_INDEX);
+    else if (j != i) ++c;
+  }
+  fwd[i * 3 + type] = c;
+  cnt[i * 3 + type] = c;
+}
+
+__global__ void csr_rev_count_kernel(const uint32_t* __restrict__ pairs, uint64_t P, int type, uint64_t n,
+                                     uint32_t* __restrict__ cnt) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += stride) {
+    const uint32_t a = pairs[2 * p], b = pairs[2 * p + 1];
+    if (b < n && a != b) atomicAdd(&cnt[static_cast<uint64_t>(b) * 3 + type], 1u);
+  }
+}
+
+__global__ void csr_fwd_fill_kernel(const uint32_t* __restrict__ pairs, uint64_t n, uint32_t k, int type,
+                                    const uint32_t* __restrict__ rp, uint32_t* __restrict__ col) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t pos = rp[i * 3 + type];
+  for (uint32_t q = 0; q < k; ++q) {
+    const uint32_t j = pairs[2 * (i * k + q) + 1];
+    if (j < n && j != i) col[pos++] = j;
+  }
+}
+
+__global__ void csr_rev_fill_kernel(const uint32_t* __restrict__ pairs, uint64_t P, int type, uint64_t n,
+                                    uint32_t* __restrict__ cursor, uint32_t* __restrict__ col) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += stride) {
+    const uint32_t a = pairs[2 * p], b = pairs[2 * p + 1];
+    if (b < n && a != b) col[atomicAdd(&cursor[static_cast<uint64_t>(b) * 3 + type], 1u)] = a;
+  }
+}
+
+__global__ void add_offsets_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint64_t len,
+                                   uint32_t* __restrict__ out) {
+  const uint64_t s = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s < len) out[s] = a[s] + b[s];
 }
 
 // Exclusive scan of u32 counts (the host checks that the total fits in u32).
@@ -146,7 +211,9 @@ __device__ __forceinline__ void bitonic_sort_range(T* s, int len, int tid, int n
   if (block) __syncthreads(); else __syncwarp();
 }
 
+// skip (may be null): the first skip[s] entries of segment s are already in their final order.
 __global__ void __launch_bounds__(SEG_WARPS * 32) seg_sort_small_kernel(const uint32_t* __restrict__ rp,
+                                                                        const uint32_t* __restrict__ skip,
                                                                         uint32_t* __restrict__ col, uint64_t nseg,
                                                                         uint32_t* __restrict__ big,
                                                                         uint32_t* __restrict__ nbig) {
@@ -154,7 +221,7 @@ __global__ void __launch_bounds__(SEG_WARPS * 32) seg_sort_small_kernel(const ui
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint64_t sidx = static_cast<uint64_t>(blockIdx.x) * SEG_WARPS + warp; sidx < nseg;
        sidx += static_cast<uint64_t>(gridDim.x) * SEG_WARPS) {
-    const uint32_t b = rp[sidx], e = rp[sidx + 1];
+    const uint32_t b = rp[sidx] + (skip ? skip[sidx] : 0u), e = rp[sidx + 1];
     const int len = static_cast<int>(e - b);
     if (len <= 1) continue;
     if (len > SEG_SMALL) {
@@ -169,12 +236,14 @@ __global__ void __launch_bounds__(SEG_WARPS * 32) seg_sort_small_kernel(const ui
   }
 }
 
-__global__ void __launch_bounds__(1024) seg_sort_mid_kernel(const uint32_t* __restrict__ rp, uint32_t* __restrict__ col,
+__global__ void __launch_bounds__(1024) seg_sort_mid_kernel(const uint32_t* __restrict__ rp,
+                                                            const uint32_t* __restrict__ skip,
+                                                            uint32_t* __restrict__ col,
                                                             const uint32_t* __restrict__ big, uint32_t nbig) {
   extern __shared__ uint32_t mbuf[];
   for (uint32_t q = blockIdx.x; q < nbig; q += gridDim.x) {
     const uint32_t sidx = big[q];
-    const uint32_t b = rp[sidx], e = rp[sidx + 1];
+    const uint32_t b = rp[sidx] + (skip ? skip[sidx] : 0u), e = rp[sidx + 1];
     const int len = static_cast<int>(e - b);
     if (len > SEG_MID) continue;
     const int P = next_pow2(len);
@@ -464,11 +533,48 @@ void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const u
   PM_CUDA(cudaMemsetAsync(cnt.get(), 0, (nseg + 1) * sizeof(uint32_t), c.stream));
   const uint32_t* lists[3] = {d_pnn, d_pmn, d_pfp};
   const uint64_t sizes[3] = {n_nn, n_mn, n_fp};
-  for (int t = 0; t < 3; ++t) {
-    if (!sizes[t]) continue;
-    const unsigned g = static_cast<unsigned>(std::min<uint64_t>(ceil_div(sizes[t], 256), c.sm_count * 16ull));
-    csr_count_kernel<<<g, 256, 0, c.stream>>>(lists[t], sizes[t], t, n, cnt.get(), c.d_err);
-    PM_LAUNCHED();
+  auto grid_for = [&](uint64_t items) {
+    return static_cast<unsigned>(std::min<uint64_t>(ceil_div(items, 256), c.sm_count * 16ull));
+  };
+  // Are the lists grouped by point (every generated list is)? Then forward entries need no atomics.
+  bool grouped = n > 0;
+  for (int t = 0; t < 3 && grouped; ++t) grouped = sizes[t] % n == 0 && sizes[t] / n < (1ull << 31);
+  DevBuf<uint32_t> flag, fwd;
+  if (grouped) {
+    flag.alloc(c, 1);
+    const uint32_t one = 1u;
+    PM_CUDA(cudaMemcpyAsync(flag.get(), &one, sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
+    for (int t = 0; t < 3; ++t) {
+      if (!sizes[t]) continue;
+      grouped_check_kernel<<<grid_for(sizes[t]), 256, 0, c.stream>>>(lists[t], sizes[t],
+                                                                     static_cast<uint32_t>(sizes[t] / n), flag.get());
+      PM_LAUNCHED();
+    }
+    uint32_t h = 0;
+    PM_CUDA(cudaMemcpyAsync(&h, flag.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+    PM_CUDA(cudaStreamSynchronize(c.stream));
+    grouped = h != 0;
+  }
+  if (grouped) {
+    fwd.alloc(c, nseg);
+    PM_CUDA(cudaMemsetAsync(fwd.get(), 0, nseg * sizeof(uint32_t), c.stream));
+    for (int t = 0; t < 3; ++t) {
+      if (!sizes[t]) continue;
+      csr_fwd_count_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(lists[t], n, static_cast<uint32_t>(sizes[t] / n), t,
+                                                                  fwd.get(), cnt.get(), c.d_err);
+      PM_LAUNCHED();
+    }
+    for (int t = 0; t < 3; ++t) {
+      if (!sizes[t]) continue;
+      csr_rev_count_kernel<<<grid_for(sizes[t]), 256, 0, c.stream>>>(lists[t], sizes[t], t, n, cnt.get());
+      PM_LAUNCHED();
+    }
+  } else {
+    for (int t = 0; t < 3; ++t) {
+      if (!sizes[t]) continue;
+      csr_count_kernel<<<grid_for(sizes[t]), 256, 0, c.stream>>>(lists[t], sizes[t], t, n, cnt.get(), c.d_err);
+      PM_LAUNCHED();
+    }
   }
   c.check_errors("pair lists");
   out.row_ptr.alloc(c, nseg + 1);
@@ -486,19 +592,38 @@ void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const u
   PM_CUDA(cudaStreamSynchronize(c.stream));
   out.entries = total;
   out.col.alloc(c, std::max<uint64_t>(total, 1));
-  // cursor = row_ptr (reuse the count buffer)
-  PM_CUDA(cudaMemcpyAsync(cnt.get(), out.row_ptr.get(), (nseg + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
-                          c.stream));
-  for (int t = 0; t < 3; ++t) {
-    if (!sizes[t]) continue;
-    const unsigned g = static_cast<unsigned>(std::min<uint64_t>(ceil_div(sizes[t], 256), c.sm_count * 16ull));
-    csr_fill_kernel<<<g, 256, 0, c.stream>>>(lists[t], sizes[t], t, n, cnt.get(), out.col.get());
+  if (grouped) {
+    // forward entries in pair order; reverse entries after them by atomics (cursor = row_ptr + forward)
+    for (int t = 0; t < 3; ++t) {
+      if (!sizes[t]) continue;
+      csr_fwd_fill_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(lists[t], n, static_cast<uint32_t>(sizes[t] / n), t,
+                                                                 out.row_ptr.get(), out.col.get());
+      PM_LAUNCHED();
+    }
+    add_offsets_kernel<<<ceil_div(nseg, 256), 256, 0, c.stream>>>(out.row_ptr.get(), fwd.get(), nseg, cnt.get());
     PM_LAUNCHED();
+    for (int t = 0; t < 3; ++t) {
+      if (!sizes[t]) continue;
+      csr_rev_fill_kernel<<<grid_for(sizes[t]), 256, 0, c.stream>>>(lists[t], sizes[t], t, n, cnt.get(),
+                                                                    out.col.get());
+      PM_LAUNCHED();
+    }
+  } else {
+    // cursor = row_ptr (reuse the count buffer)
+    PM_CUDA(cudaMemcpyAsync(cnt.get(), out.row_ptr.get(), (nseg + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                            c.stream));
+    for (int t = 0; t < 3; ++t) {
+      if (!sizes[t]) continue;
+      csr_fill_kernel<<<grid_for(sizes[t]), 256, 0, c.stream>>>(lists[t], sizes[t], t, n, cnt.get(), out.col.get());
+      PM_LAUNCHED();
+    }
   }
+  // sort what the atomics placed: whole segments, or (grouped) the reverse part after the forward entries
+  const uint32_t* skip = grouped ? fwd.get() : nullptr;
   DevBuf<uint32_t> big(c, nseg + 1);
   PM_CUDA(cudaMemsetAsync(big.get() + nseg, 0, sizeof(uint32_t), c.stream));
   const unsigned g = static_cast<unsigned>(std::min<uint64_t>(ceil_div(nseg, SEG_WARPS), c.sm_count * 8ull));
-  seg_sort_small_kernel<<<g, SEG_WARPS * 32, 0, c.stream>>>(out.row_ptr.get(), out.col.get(), nseg, big.get(),
+  seg_sort_small_kernel<<<g, SEG_WARPS * 32, 0, c.stream>>>(out.row_ptr.get(), skip, out.col.get(), nseg, big.get(),
                                                            big.get() + nseg);
   PM_LAUNCHED();
   uint32_t nbig = 0;
@@ -509,18 +634,21 @@ void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const u
     PM_CUDA(cudaFuncSetAttribute(seg_sort_mid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
     seg_sort_mid_kernel<<<std::min<uint32_t>(nbig, c.sm_count * 2), 1024, smem, c.stream>>>(
-        out.row_ptr.get(), out.col.get(), big.get(), nbig);
+        out.row_ptr.get(), skip, out.col.get(), big.get(), nbig);
     PM_LAUNCHED();
     // Segments longer than shared memory (points that appear in > 32768 pairs of one type).
-    std::vector<uint32_t> hb(nbig), hrp;
+    std::vector<uint32_t> hb(nbig), hrp(nseg + 1), hskip;
     PM_CUDA(cudaMemcpyAsync(hb.data(), big.get(), nbig * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
-    hrp.resize(nseg + 1);
     PM_CUDA(cudaMemcpyAsync(hrp.data(), out.row_ptr.get(), (nseg + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                             c.stream));
+    if (skip) {
+      hskip.resize(nseg);
+      PM_CUDA(cudaMemcpyAsync(hskip.data(), skip, nseg * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+    }
     PM_CUDA(cudaStreamSynchronize(c.stream));
     DevBuf<uint32_t> scratch;
     for (uint32_t q = 0; q < nbig; ++q) {
-      const uint32_t b = hrp[hb[q]], len = hrp[hb[q] + 1] - b;
+      const uint32_t b = hrp[hb[q]] + (skip ? hskip[hb[q]] : 0u), len = hrp[hb[q] + 1] - b;
       if (len <= static_cast<uint32_t>(SEG_MID)) continue;
       const uint32_t P = static_cast<uint32_t>(next_pow2(static_cast<int>(len)));
       if (scratch.count < P) scratch.alloc(c, P);
