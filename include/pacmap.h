@@ -307,8 +307,9 @@ pacmap_status pacmap_preprocess_noalloc(const float* d_x, uint64_t n, uint64_t d
  * with CUDA events on its stream. pacmap_stage_times fills up to `cap` values in milliseconds, in the
  * order preprocess, knn, reselect, sample_mn, sample_fp, csr, init, optimize (then, when the tensor-core
  * kNN ran: its filter kernel alone, the number of rows it left to the exact fallback, the time of the
- * tile pruning's bound pass and lists, and the (row block, column tile) pairs computed, of the full
- * sweep, and of the bound pass), and returns how many. */
+ * tile pruning's bound pass and lists, the (row block, column tile) pairs computed, of the full
+ * sweep, and of the bound pass, and per row: candidate entries written by the filter passes, compactions
+ * inside them, and candidates left for the exact re-rank), and returns how many. */
 void pacmap_set_stage_timing(int32_t enabled);
 uint64_t pacmap_stage_times(double* out_ms, uint64_t cap);
 

@@ -185,13 +185,17 @@ void generate_pairs_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, co
   if (tm) tm->stop(ST_KNN);
   if (tm && tm->on) {
     const KnnTcStats& ks = last_tc_stats();
-    g_stage_ms.resize(ST_COUNT + 6, 0.0);
+    g_stage_ms.resize(ST_COUNT + 9, 0.0);
     g_stage_ms[ST_COUNT] = ks.filter_ms;
     g_stage_ms[ST_COUNT + 1] = static_cast<double>(ks.fallback_rows);
     g_stage_ms[ST_COUNT + 2] = ks.bound_ms;
     g_stage_ms[ST_COUNT + 3] = static_cast<double>(ks.tiles_visited);
     g_stage_ms[ST_COUNT + 4] = static_cast<double>(ks.tiles_full);
     g_stage_ms[ST_COUNT + 5] = static_cast<double>(ks.tiles_bound);
+    const double rows = ks.rows ? static_cast<double>(ks.rows) : 1.0;
+    g_stage_ms[ST_COUNT + 6] = static_cast<double>(ks.insertions) / rows;
+    g_stage_ms[ST_COUNT + 7] = static_cast<double>(ks.compactions) / rows;
+    g_stage_ms[ST_COUNT + 8] = static_cast<double>(ks.band_entries) / rows;
   }
   if (tm) tm->start(ST_RESELECT);
   sigma_device(c, dist.get(), n, kp, sig.get());

@@ -209,6 +209,26 @@ struct WarpStream {
 constexpr uint64_t SAMPLE_ATTEMPT_CAP = 1ull << 26;
 
 // ---------------------------------------------------------------------------------------------
+// Packed two-wide f32 arithmetic (sm_100: one instruction for two round-to-nearest operations); a
+// pair lives in one 64-bit register, element 0 in the low half.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t f32x2_pack(float2 v) {
+  return static_cast<uint64_t>(__float_as_uint(v.x)) | (static_cast<uint64_t>(__float_as_uint(v.y)) << 32);
+}
+__device__ __forceinline__ float f32x2_lo(uint64_t v) { return __uint_as_float(static_cast<uint32_t>(v)); }
+__device__ __forceinline__ float f32x2_hi(uint64_t v) { return __uint_as_float(static_cast<uint32_t>(v >> 32)); }
+__device__ __forceinline__ uint64_t f32x2_sub(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f32x2_fma(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Warp helpers.
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }

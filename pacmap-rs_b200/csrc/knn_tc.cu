@@ -74,6 +74,7 @@ enum FilterMode { MODE_TILE = 0, MODE_KBLOCK = 1, MODE_STREAM = 2 };
 constexpr uint64_t PRUNE_MIN_ROWS = 32768;  // tile pruning from 256 column tiles on
 constexpr int PRUNE_PROBE = 2;              // the bound pass: own cells (+ the nearest cell of a small one)
 constexpr int TC_SMEM_LIMIT = 232448;  // 227 KB of dynamic shared memory per block
+constexpr int FILTER_SLACK = 8;        // the filter's compactions settle for a key within rank + 8 entries
 template <int KB, int MODE>
 struct FilterLayout {
   static constexpr int A_RES = MODE == MODE_STREAM ? 0 : 2 * KB * KB_BYTES;
@@ -127,10 +128,13 @@ __device__ __forceinline__ void load_row(const uint2* __restrict__ cand, int m, 
 // back in order. With ge (the separate compaction kernels) v = u - 4 e_j is recovered exactly up to one
 // rounding (kept when within 2^-22 of the magnitudes above theta); without it (inside the filter, where
 // a gather per entry would stall the epilogue) an entry is kept when u <= theta + e4max, a superset.
+// slack > 0 ends the bisection at the first key T with rank <= #{keys <= T} <= rank + slack: T is then
+// at or above the rank-th smallest key, so theta still bounds the row's k'-th neighbour (a looser bound
+// for fewer serial steps; the filter's compactions use it, the final one is exact).
 template <int PER>
 __device__ __forceinline__ int compact_row(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
                                            const RowRegs<PER>& r, float e4max, const float2* __restrict__ ge,
-                                           float& theta_out, uint32_t* ukey_out = nullptr) {
+                                           float& theta_out, uint32_t* ukey_out = nullptr, int slack = 0) {
   const int lane = threadIdx.x & 31;
   uint32_t rk[PER];
   uint32_t kmin = 0xFFFFFFFFu, kmax = 0u;
@@ -144,7 +148,8 @@ __device__ __forceinline__ int compact_row(uint2* __restrict__ cand, int m, int 
     }
   }
   // The rank-th smallest key by bisection on [min key, max key] with warp-wide counts (no shared
-  // memory, no atomics): the smallest key value T with #{keys <= T} >= rank.
+  // memory, no atomics): the smallest key value T with #{keys <= T} >= rank. #{keys <= hi} >= rank holds
+  // throughout, so stopping early (slack) leaves hi a valid threshold key.
   uint32_t lo = __reduce_min_sync(0xFFFFFFFFu, kmin), hi = __reduce_max_sync(0xFFFFFFFFu, kmax);
   while (lo < hi) {
     const uint32_t mid = lo + ((hi - lo) >> 1);
@@ -152,10 +157,14 @@ __device__ __forceinline__ int compact_row(uint2* __restrict__ cand, int m, int 
 #pragma unroll
     for (int q = 0; q < PER; ++q) cnt += (rk[q] <= mid) ? 1u : 0u;
     cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
-    if (cnt >= static_cast<uint32_t>(rank)) hi = mid;
-    else lo = mid + 1u;
+    if (cnt >= static_cast<uint32_t>(rank)) {
+      hi = mid;
+      if (cnt <= static_cast<uint32_t>(rank + slack) && slack > 0) break;
+    } else {
+      lo = mid + 1u;
+    }
   }
-  const uint32_t prefix = lo;
+  const uint32_t prefix = hi;
   const float th = theta_from(prefix, n_i, e4_i);
   float e4j[PER];
   if (ge) {
@@ -530,7 +539,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const uint32_t* __restrict__ perm, int rank, uint2* __restrict__ cand, int* __restrict__ cand_cnt,
     uint32_t* __restrict__ overflow_rows, uint32_t* __restrict__ n_overflow, uint32_t* __restrict__ err,
     int block_offset, const uint32_t* __restrict__ tile_ptr, const uint32_t* __restrict__ tile_list,
-    const float* __restrict__ resume_theta, const uint32_t* __restrict__ e4max_bits) {
+    const float* __restrict__ resume_theta, const uint32_t* __restrict__ e4max_bits,
+    unsigned long long* __restrict__ counters) {
   using L = FilterLayout<KB, MODE>;
   constexpr int NST = L::NST;
   constexpr int C = 32 * PER;
@@ -733,6 +743,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const uint64_t cbase = row * static_cast<uint64_t>(C);
     const float e4max = __uint_as_float(*e4max_bits);
     bool ok = true;
+    uint32_t n_ins = 0, n_comp = 0;  // this row's insertions and compactions (statistics)
     auto screen = [&](const uint32_t (&r)[32], int colb) {
       float m8[4];
 #pragma unroll
@@ -752,6 +763,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
                 const uint32_t col = static_cast<uint32_t>(colb + c);
                 cand[cbase + cnt] = make_uint2(col, __float_as_uint(v + __ldg(&ge[col].y)));
                 ++cnt;
+                ++n_ins;
               }
             }
           }
@@ -799,10 +811,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
           const float nL = __shfl_sync(0xFFFFFFFFu, n_i, L);
           const float eL = __shfl_sync(0xFFFFFFFFu, e4_i, L);
           float th;
-          const int kept = compact_row<PER>(cand + rb, m, min(rank, m), nL, eL, cur, e4max, nullptr, th);
+          const int kept = compact_row<PER>(cand + rb, m, min(rank, m), nL, eL, cur, e4max, nullptr, th, nullptr,
+                                            FILTER_SLACK);
           if (lane == L) {
             theta = th;
             cnt = kept;
+            ++n_comp;
             if (cnt > C - TC_BN) {  // the band does not fit: exact recomputation later
               theta = -__int_as_float(0x7f800000);
               cnt = 0;
@@ -823,6 +837,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
       sh->abort_flag = 1;
     }
     if (valid) cand_cnt[row] = (theta == -__int_as_float(0x7f800000)) ? -1 : cnt;
+    if (counters) {
+      const uint32_t wi = __reduce_add_sync(0xFFFFFFFFu, n_ins), wc = __reduce_add_sync(0xFFFFFFFFu, n_comp);
+      if (lane == 0) {
+        atomicAdd(&counters[0], static_cast<unsigned long long>(wi));
+        atomicAdd(&counters[1], static_cast<unsigned long long>(wc));
+      }
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -846,9 +867,11 @@ constexpr int RC_WARPS = 4;
 template <int PER>
 __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     uint64_t n, int rank, const float* __restrict__ nrm, const float2* __restrict__ ge, uint2* __restrict__ cand,
-    int* __restrict__ cand_cnt, float* __restrict__ ub, float* __restrict__ theta_out) {
+    int* __restrict__ cand_cnt, float* __restrict__ ub, float* __restrict__ theta_out,
+    unsigned long long* __restrict__ band_total) {
   constexpr int C = 32 * PER;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned long long band = 0;
   for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * RC_WARPS + warp; r < n;
        r += static_cast<uint64_t>(gridDim.x) * RC_WARPS) {
     const int m0 = min(cand_cnt[r], C);
@@ -864,6 +887,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     RowRegs<PER> regs;
     load_row<PER>(cand + rb, m0, regs);
     const int m = compact_row<PER>(cand + rb, m0, min(rank, m0), n_i, e4_i, regs, 0.0f, ge, th, &ukey);
+    band += static_cast<unsigned long long>(m);
     if (lane == 0) {
       cand_cnt[r] = m;
       if (theta_out) theta_out[r] = th;
@@ -875,6 +899,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
       }
     }
   }
+  if (band_total && lane == 0 && band) atomicAdd(band_total, band);
 }
 
 // 3b. exact re-rank of the compacted band: the reference's f32 distance of every survivor (8-lane
@@ -1178,6 +1203,9 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
 
   DevBuf<uint2> cand(c, n_pad * C);
   DevBuf<int> ccnt(c, n_pad);
+  // statistics: insertions and compactions of the filter passes, entries of the final bands
+  DevBuf<unsigned long long> counters(c, 3);
+  PM_CUDA(cudaMemsetAsync(counters.get(), 0, 3 * sizeof(unsigned long long), c.stream));
   DevBuf<uint32_t> ovf(c, n + 1), fbk(c, n + 1);
 
   const uint32_t idesc = idesc_f16(bf16);
@@ -1200,7 +1228,8 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
       if (grid == 0) return;
       kern<<<grid, TC_THREADS, smem, c.stream>>>(map, gmap, n, n_pad, KB, idesc, ge.get(), nrm.get(), perm.get(), rank,
                                                  cand.get(), ccnt.get(), ovf_rows, n_ovf, c.d_err,
-                                                 static_cast<int>(blk0), lptr, llist, resume_theta, e4max.get());
+                                                 static_cast<int>(blk0), lptr, llist, resume_theta, e4max.get(),
+                                                 counters.get());
     };
     const bool p16 = PER == 16;
     if (mode == MODE_STREAM) {
@@ -1227,13 +1256,13 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     PM_LAUNCHED();
   };
   const unsigned cgrid = std::min<unsigned>(ceil_div(n, RC_WARPS), c.sm_count * 16);
-  auto compact = [&](float* ub, float* theta_out) {
+  auto compact = [&](float* ub, float* theta_out, unsigned long long* band_total) {
     if (PER == 16)
       knn_compact_kernel<16><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get(),
-                                                                    ub, theta_out);
+                                                                    ub, theta_out, band_total);
     else
       knn_compact_kernel<32><<<cgrid, RC_WARPS * 32, 0, c.stream>>>(n, rank, nrm.get(), ge.get(), cand.get(), ccnt.get(),
-                                                                    ub, theta_out);
+                                                                    ub, theta_out, band_total);
     PM_LAUNCHED();
   };
   cudaEvent_t ev[3];
@@ -1256,7 +1285,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     c.check_errors("tensor-core kNN bound pass");
     DevBuf<float> ub(c, n_pad);
     resume.alloc(c, n_pad);
-    compact(ub.get(), resume.get());
+    compact(ub.get(), resume.get(), nullptr);
     PruneInputs in;
     in.perm = perm.get();
     in.cell = cell.get();
@@ -1285,7 +1314,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   st.filter_ms = fms;
   st.bound_ms = bms;
 
-  compact(nullptr, nullptr);
+  compact(nullptr, nullptr, counters.get() + 2);
   const int di = static_cast<int>(d), ki = static_cast<int>(kp);
   auto rerank = [&](auto kern, int warps) {
     const unsigned rgrid = std::min<unsigned>(ceil_div(n, warps), c.sm_count * 32);
@@ -1307,10 +1336,16 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
 
   // Rows the filter could not settle: exact SIMT recomputation, scattered into place.
   uint32_t counts[2] = {0, 0};
+  unsigned long long cv[3] = {0, 0, 0};
   PM_CUDA(cudaMemcpyAsync(&counts[0], ovf.get() + n, 4, cudaMemcpyDeviceToHost, c.stream));
   PM_CUDA(cudaMemcpyAsync(&counts[1], fbk.get() + n, 4, cudaMemcpyDeviceToHost, c.stream));
+  PM_CUDA(cudaMemcpyAsync(cv, counters.get(), sizeof(cv), cudaMemcpyDeviceToHost, c.stream));
   PM_CUDA(cudaStreamSynchronize(c.stream));
   st.fallback_rows = counts[0] + counts[1];
+  st.insertions = cv[0];
+  st.compactions = cv[1];
+  st.band_entries = cv[2];
+  st.rows = n;
   const uint32_t* lists[2] = {ovf.get(), fbk.get()};
   for (int q = 0; q < 2; ++q) {
     if (!counts[q]) continue;

@@ -19,6 +19,10 @@ struct KnnTcStats {
   uint64_t tiles_full = 0;      // (row block, column tile) pairs of the full sweep
   uint64_t tiles_visited = 0;   // pairs the filter computed
   uint64_t tiles_bound = 0;     // pairs the bound pass computed
+  uint64_t insertions = 0;      // candidate entries the filter passes wrote (all rows)
+  uint64_t compactions = 0;     // row compactions inside the filter passes
+  uint64_t band_entries = 0;    // candidates left for the exact re-rank (all rows)
+  uint64_t rows = 0;            // rows of the problem
 };
 KnnTcStats& last_tc_stats();
 }  // namespace pacmap

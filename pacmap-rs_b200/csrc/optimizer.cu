@@ -3,9 +3,9 @@
 //
 // K7 build_csr: every pair (i, j), i != j, of the three lists becomes two entries -- partner j in the
 //    segment (i, type) and partner i in the segment (j, type) -- via a counting sort, then each segment
-//    is sorted by partner. When the lists are grouped by point (the generated ones are), a segment is
-//    point i's own partners in pair order followed by the points that drew i, sorted: only that second
-//    part is placed by atomics and sorted. A pair's contribution to each endpoint is bit-identical whichever endpoint
+//    is sorted by partner. When the lists are grouped by point (the generated ones are), a mid-near or
+//    far segment is point i's own partners in pair order followed by the points that drew i, sorted:
+//    only that second part is placed by atomics and sorted (a neighbour segment is sorted whole). A pair's contribution to each endpoint is bit-identical whichever endpoint
 //    lists it (the squared distance and the weight use |y_i - y_j| only), so the sorted segments fix
 //    one deterministic summation order with no floating-point atomics. (The reference's rayon reduce,
 //    gradient.rs:53-70, has no fixed order at all.)
@@ -211,7 +211,14 @@ __device__ __forceinline__ void bitonic_sort_range(T* s, int len, int tid, int n
   if (block) __syncthreads(); else __syncwarp();
 }
 
-// skip (may be null): the first skip[s] entries of segment s are already in their final order.
+// skip (may be null): the first skip[s] entries of segment s are already in their final order. The
+// neighbour segments (type 0) are sorted whole all the same: a point and its neighbour are often each
+// other's neighbours, and sorting puts the two entries of such a pair side by side, where the gradient
+// kernel's lanes read the partner's coordinates in one request instead of two.
+__device__ __forceinline__ uint32_t seg_skip(const uint32_t* __restrict__ skip, uint64_t sidx) {
+  return (skip && sidx % 3 != 0) ? skip[sidx] : 0u;
+}
+
 __global__ void __launch_bounds__(SEG_WARPS * 32) seg_sort_small_kernel(const uint32_t* __restrict__ rp,
                                                                         const uint32_t* __restrict__ skip,
                                                                         uint32_t* __restrict__ col, uint64_t nseg,
@@ -221,7 +228,7 @@ __global__ void __launch_bounds__(SEG_WARPS * 32) seg_sort_small_kernel(const ui
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint64_t sidx = static_cast<uint64_t>(blockIdx.x) * SEG_WARPS + warp; sidx < nseg;
        sidx += static_cast<uint64_t>(gridDim.x) * SEG_WARPS) {
-    const uint32_t b = rp[sidx] + (skip ? skip[sidx] : 0u), e = rp[sidx + 1];
+    const uint32_t b = rp[sidx] + seg_skip(skip, sidx), e = rp[sidx + 1];
     const int len = static_cast<int>(e - b);
     if (len <= 1) continue;
     if (len > SEG_SMALL) {
@@ -243,7 +250,7 @@ __global__ void __launch_bounds__(1024) seg_sort_mid_kernel(const uint32_t* __re
   extern __shared__ uint32_t mbuf[];
   for (uint32_t q = blockIdx.x; q < nbig; q += gridDim.x) {
     const uint32_t sidx = big[q];
-    const uint32_t b = rp[sidx] + (skip ? skip[sidx] : 0u), e = rp[sidx + 1];
+    const uint32_t b = rp[sidx] + seg_skip(skip, sidx), e = rp[sidx + 1];
     const int len = static_cast<int>(e - b);
     if (len > SEG_MID) continue;
     const int P = next_pow2(len);
@@ -648,7 +655,7 @@ void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const u
     PM_CUDA(cudaStreamSynchronize(c.stream));
     DevBuf<uint32_t> scratch;
     for (uint32_t q = 0; q < nbig; ++q) {
-      const uint32_t b = hrp[hb[q]] + (skip ? hskip[hb[q]] : 0u), len = hrp[hb[q] + 1] - b;
+      const uint32_t b = hrp[hb[q]] + ((skip && hb[q] % 3 != 0) ? hskip[hb[q]] : 0u), len = hrp[hb[q] + 1] - b;
       if (len <= static_cast<uint32_t>(SEG_MID)) continue;
       const uint32_t P = static_cast<uint32_t>(next_pow2(static_cast<int>(len)));
       if (scratch.count < P) scratch.alloc(c, P);

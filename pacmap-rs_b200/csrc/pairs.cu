@@ -372,6 +372,65 @@ __global__ void sample_mn_kernel(const float* __restrict__ x, uint64_t n, int d,
 // words, so the picks are the rule's picks. Otherwise (rare: about 120 * n_mn / n per point) the point
 // is redone by the sequential rule. Candidates and distances are staged in shared memory.
 constexpr int MS_WARPS = 8, MS_MAXC = 32 * 6;
+constexpr uint32_t MN_DRAW_BATCHES = 4;  // 512 words: 6 n_mn <= 192 draws need fewer unless n is tiny
+
+// The rule's draws of all n_mn slots (6 candidates each) by the whole warp at once: lane L turns the four
+// words of Philox block base + L into candidates (uniform by rejection, as PointStream::uniform, and the
+// point itself skipped), and a prefix count over the lanes gives every accepted word its draw number, so
+// draw p is the p-th accepted word -- the candidate the sequential loop assigns to slot p / 6, position
+// p % 6, as long as no slot draws a point twice (the loop would skip the repeat and shift every later
+// draw). Returns false when a slot holds a repeat or the batches ran out: the caller then runs the
+// sequential rule for the point. cs receives 6 n_mn candidates in slot order.
+__device__ __forceinline__ bool mn_draw_parallel(uint64_t seed, uint64_t i, uint32_t n, uint32_t n_mn,
+                                                 uint32_t* __restrict__ cs) {
+  const uint32_t lane = lane_id();
+  const uint32_t total = n_mn * 6;
+  const uint32_t zone = (n << __clz(n)) - 1u;
+  const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
+  const uint32_t c1 = static_cast<uint32_t>(i), c2 = static_cast<uint32_t>(i >> 32);
+  uint32_t have = 0;
+  for (uint32_t b = 0; b < MN_DRAW_BATCHES && have < total; ++b) {
+    uint32_t w[4];
+    philox4x32_10(b * 32u + lane, c1, c2, TAG_SAMPLE, k0, k1, w);
+    uint32_t val[4], okm = 0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      val[t] = __umulhi(w[t], n);
+      const bool ok = (w[t] * n <= zone) && (val[t] != static_cast<uint32_t>(i));
+      okm |= (ok ? 1u : 0u) << t;
+    }
+    const uint32_t cnt = static_cast<uint32_t>(__popc(okm));
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= static_cast<uint32_t>(o)) incl += v;
+    }
+    uint32_t p = have + incl - cnt;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      if ((okm >> t) & 1u) {
+        if (p < total) cs[p] = val[t];
+        ++p;
+      }
+    }
+    have += __shfl_sync(0xFFFFFFFFu, incl, 31);
+  }
+  __syncwarp();
+  if (have < total) return false;
+  bool dup = false;
+  for (uint32_t sl = lane; sl < n_mn; sl += 32) {
+    uint32_t c[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) c[t] = cs[sl * 6 + t];
+#pragma unroll
+    for (int a = 0; a < 6; ++a)
+#pragma unroll
+      for (int b = a + 1; b < 6; ++b) dup |= c[a] == c[b];
+  }
+  return !__any_sync(0xFFFFFFFFu, dup);
+}
+
 template <int NC>
 __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_spec_kernel(const float* __restrict__ x, uint64_t n, int d,
                                                                       uint32_t n_mn, uint64_t seed,
@@ -390,35 +449,9 @@ __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_spec_kernel(const flo
   uint32_t* cs = s_cand[warp];
   float* ds = s_dist[warp];
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * MS_WARPS + warp; i < n; i += warps) {
-    // 1. every slot's draws (self and repeats within the slot rejected, as in the rule)
-    WarpStream s(seed, i);
-    uint64_t budget = SAMPLE_ATTEMPT_CAP;
-    bool failed = false;
-    for (uint32_t jslot = 0; jslot < n_mn && !failed; ++jslot) {
-      uint32_t cand[6] = {0, 0, 0, 0, 0, 0};
-      uint32_t cnt = 0;
-      while (cnt < 6) {
-        uint32_t j;
-        if (!s.uniform(static_cast<uint32_t>(n), j, budget)) {
-          failed = true;
-          break;
-        }
-        if (j == i) continue;
-        bool dup = false;
-#pragma unroll
-        for (int t = 0; t < 6; ++t) dup |= (t < static_cast<int>(cnt) && cand[t] == j);
-        if (dup) continue;
-#pragma unroll
-        for (int t = 0; t < 6; ++t)
-          if (t == static_cast<int>(cnt)) cand[t] = j;
-        ++cnt;
-      }
-#pragma unroll
-      for (int t = 0; t < 6; ++t)
-        if (static_cast<int>(lane) == t) cs[jslot * 6 + t] = cand[t];
-    }
-    __syncwarp();
-    if (failed) {  // the sequential rule reports the failure
+    // 1. every slot's draws (self and repeats within the slot rejected, as in the rule), all words at once;
+    //    a repeat within a slot (or words beyond the parallel batches) sends the point to the sequential rule
+    if (!mn_draw_parallel(seed, i, static_cast<uint32_t>(n), n_mn, cs)) {
       mn_point_sequential(x, n, d, n_mn, seed, i, out, err);
       continue;
     }
@@ -534,35 +567,9 @@ __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_screen_kernel(
   float* lo_s = s_lo[warp];
   float* hi_s = s_hi[warp];
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * MS_WARPS + warp; i < n; i += warps) {
-    // 1. every slot's draws (self and repeats within the slot rejected, as in the rule)
-    WarpStream s(seed, i);
-    uint64_t budget = SAMPLE_ATTEMPT_CAP;
-    bool failed = false;
-    for (uint32_t jslot = 0; jslot < n_mn && !failed; ++jslot) {
-      uint32_t cand[6] = {0, 0, 0, 0, 0, 0};
-      uint32_t cnt = 0;
-      while (cnt < 6) {
-        uint32_t j;
-        if (!s.uniform(static_cast<uint32_t>(n), j, budget)) {
-          failed = true;
-          break;
-        }
-        if (j == i) continue;
-        bool dup = false;
-#pragma unroll
-        for (int t = 0; t < 6; ++t) dup |= (t < static_cast<int>(cnt) && cand[t] == j);
-        if (dup) continue;
-#pragma unroll
-        for (int t = 0; t < 6; ++t)
-          if (t == static_cast<int>(cnt)) cand[t] = j;
-        ++cnt;
-      }
-#pragma unroll
-      for (int t = 0; t < 6; ++t)
-        if (static_cast<int>(lane) == t) cs[jslot * 6 + t] = cand[t];
-    }
-    __syncwarp();
-    if (failed) {  // the sequential rule reports the failure
+    // 1. every slot's draws (self and repeats within the slot rejected, as in the rule), all words at once;
+    //    a repeat within a slot (or words beyond the parallel batches) sends the point to the sequential rule
+    if (!mn_draw_parallel(seed, i, static_cast<uint32_t>(n), n_mn, cs)) {
       mn_point_sequential(x, n, d, n_mn, seed, i, out, err);
       continue;
     }
@@ -577,11 +584,12 @@ __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_screen_kernel(
       }
       for (int c = static_cast<int>(lane); c < total; c += 32) asm volatile("prefetch.global.L2 [%0];" ::"l"(eps + cs[c]));
     }
-    // 2. screening distances on the fp16 rows: lane l8 of a group holds E consecutive elements
+    // 2. screening distances on the fp16 rows: lane l8 of a group holds E consecutive elements (as E / 2
+    //    pairs for the packed two-wide f32 arithmetic: even and odd elements are summed separately)
     const float* a = x + i * d;
-    float xe[E];
+    uint64_t xe[E / 2];
 #pragma unroll
-    for (int q = 0; q < E; ++q) xe[q] = a[l8 * E + q];
+    for (int q = 0; q < E / 2; ++q) xe[q] = *reinterpret_cast<const uint64_t*>(a + l8 * E + 2 * q);
     for (int c0 = 0; c0 < total; c0 += 8) {
       const int ca = c0 + grp, cb = c0 + 4 + grp;
       const uint32_t ja = ca < total ? cs[ca] : static_cast<uint32_t>(i);
@@ -595,7 +603,7 @@ __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_screen_kernel(
         vb[q] = pb[q];
       }
       const float ea = eps[ja], eb = eps[jb];
-      float sa = 0.0f, sb = 0.0f;
+      uint64_t pa2 = 0, pb2 = 0;  // (even, odd) partial sums
 #pragma unroll
       for (int q = 0; q < E / 8; ++q) {
         const __half2* ha = reinterpret_cast<const __half2*>(&va[q]);
@@ -603,12 +611,12 @@ __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_screen_kernel(
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
           const float2 fa = __half22float2(ha[w]), fb = __half22float2(hb[w]);
-          const float a0 = xe[8 * q + 2 * w] - fa.x, a1 = xe[8 * q + 2 * w + 1] - fa.y;
-          const float b0 = xe[8 * q + 2 * w] - fb.x, b1 = xe[8 * q + 2 * w + 1] - fb.y;
-          sa = fmaf(a0, a0, fmaf(a1, a1, sa));
-          sb = fmaf(b0, b0, fmaf(b1, b1, sb));
+          const uint64_t da2 = f32x2_sub(xe[4 * q + w], f32x2_pack(fa)), db2 = f32x2_sub(xe[4 * q + w], f32x2_pack(fb));
+          pa2 = f32x2_fma(da2, da2, pa2);
+          pb2 = f32x2_fma(db2, db2, pb2);
         }
       }
+      float sa = f32x2_lo(pa2) + f32x2_hi(pa2), sb = f32x2_lo(pb2) + f32x2_hi(pb2);
 #pragma unroll
       for (int o = 4; o > 0; o >>= 1) {
         sa += __shfl_xor_sync(0xFFFFFFFFu, sa, o);
@@ -616,7 +624,9 @@ __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_screen_kernel(
       }
       if (l8 == 0) {
         const float da = sqrtf(sa), db = sqrtf(sb);
-        // |ref - true| <= (d/8 + 12) 2^-24 true and |da - |x_i - h_j|| <= (d + 4) 2^-25 da: 2^-15 covers both
+        // |ref - true| <= (d/8 + 12) 2^-24 true and |da - |x_i - h_j|| <= (d/2 + 8) 2^-24 da (two fused
+        // multiply-add chains of d/16 terms per lane, 8 lanes, 3 shuffle sums, the final add, sqrt): 2^-15
+        // covers both
         if (ca < total) {
           lo_s[ca] = da * (1.0f - MN_REL) - ea * (1.0f + MN_REL);
           hi_s[ca] = (da + ea) * (1.0f + MN_REL);
