@@ -53,9 +53,11 @@ WORKLOADS = {
 }
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant kernels at the
-# 1,000,000 x 128 workload, from one ncu capture each (the kernel's profile summary gives the command);
-# None until captured.
-TRAFFIC = {"knn_filter_kernel": None, "grad_adam_kernel": None}
+# 1,000,000 x 128 workload, from one-pass captures (ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
+# -k regex:<kernel> -s <launches to skip> on `bench.py --minimal --steps 1 --warmup 1`): the filter's main
+# pass (the launch its roofline times; the bound pass moves 15.4 GB, mostly candidate writes), and the
+# gradient's average over the (0, 50, 150) schedule (1.182 GB per phase-2 launch, 1.143 GB per phase-3).
+TRAFFIC = {"knn_filter_kernel": 5374556672, "grad_adam_kernel": 1152481088}
 
 
 def _peaks():
@@ -285,7 +287,9 @@ def run_ours(args, rank, world, local_rank):
     # of n_train draws, then AdamW on (x', embedding)
     train_s, train_losses, train_fit_s, tstats = None, None, None, None
     if args.minimal:
+        # untrained weights, mapped with unit statistics: the same kernels as the trained run
         params = learned.init_params(d, dim, seed=0)
+        tstats = (np.zeros(dim, np.float32), np.ones(dim, np.float32))
     else:
         x_train = make_data(n_train, d, seed=0, draw_seed=10_000 + rank, generator=gen)
         torch.cuda.synchronize()
@@ -389,6 +393,17 @@ def run_ours(args, rank, world, local_rank):
     if gate["continued"]:
         step_learned()
         q_final = pm.quality(x, dy_c.cpu().numpy(), sample, trip, 10, local_rank)
+    # the optimiser's own objective at the end (phase-3 weights w_nn = 1, w_mn = 0, w_fp = 1) on the pairs
+    # both runs share (same draw, same seed): it separates embeddings that the two metrics above do not
+    # (the network's prediction alone, no iterations, passes both)
+    cfg_pred = pm.Configuration(seed=7, num_iters=(0, 0, 0), embedding_dimensions=dim, device=local_rank)
+    dy_0 = torch.empty((n, dim), dtype=torch.float32, device=dev)
+    learned.fit_transform_learned_device(dx.data_ptr(), n, d, dy_0.data_ptr(), params, cfg_pred, target_stats=tstats)
+    q_pred = pm.quality(x, dy_0.cpu().numpy(), sample, trip, 10, local_rank)
+    pnn, pmn, pfp = pm.stages.generate_pairs(x, cfg_plain)
+    loss3 = {name: round(float(pm.stages.gradient(y.cpu().numpy(), pnn, pmn, pfp, 1.0, 0.0, 1.0, local_rank)[-1, 0]), 1)
+             for name, y in (("plain", dy_p), ("learned_short", dy_l), ("prediction_only", dy_0))}
+    del pnn, pmn, pfp, dy_0
     # stage breakdown of one untimed step of each (CUDA events inside the library, on its stream)
     pm.set_stage_timing(True)
     step_plain()
@@ -403,6 +418,8 @@ def run_ours(args, rank, world, local_rank):
     launches = pm.last_launch_count()
     ms_plain = timed(step_plain, args.steps)
     e2e_steps = max(1, args.steps // 2)
+    for _ in range(args.warmup):
+        step_e2e()
     ms_e2e = timed(step_e2e, e2e_steps)
 
     if rank != 0:
@@ -464,9 +481,12 @@ def run_ours(args, rank, world, local_rank):
         "gate": {"rule": ("continue on the plain schedule if 10-NN preservation or triplet accuracy is more than "
                           "0.005 below the plain run's"),
                  "continued": gate["continued"], "plain": rnd(q_plain), "learned_short": rnd(q_learned),
-                 "final": rnd(q_final), "random_embedding": rnd(q_random),
+                 "final": rnd(q_final), "random_embedding": rnd(q_random), "prediction_only": rnd(q_pred),
+                 "phase3_objective": loss3,
                  "note": ("10-NN preservation of this generator's embeddings is near chance (clusters of ~20,000 "
-                          "Gaussian points have no 2-D local structure); triplet accuracy discriminates")},
+                          "Gaussian points have no 2-D local structure) and triplet accuracy measures global order "
+                          "only: the network's prediction with no iterations passes both. phase3_objective is the "
+                          "optimiser's loss (lower is better) on the shared pairs")},
         "mlp_train_s": round(train_s, 3) if train_s else None,
         "train_fit_s": round(train_fit_s, 3) if train_fit_s else None,
         "mlp_train_loss": [round(float(v), 4) for v in (train_losses[0], train_losses[-1])] if train_losses is not None else None,
