@@ -604,7 +604,7 @@ void mlp_apply_device(Ctx& c, const float* params, uint64_t d, uint64_t dim, con
   MlpNet net;
   net.alloc(c, static_cast<int>(d), static_cast<int>(dim));
   net.upload(c, params);
-  const uint64_t chunk = 1ull << 18;  // rows per pass (bounded scratch)
+  const uint64_t chunk = 1ull << 20;  // rows per pass (bounded scratch: 2.3 GB at d = 128)
   DevBuf<__nv_bfloat16> X(c, chunk * net.dp), H1(c, chunk * MLP_H), H2(c, chunk * MLP_H);
   DevBuf<float> out(c, chunk * net.dp16);
   for (uint64_t r0 = 0; r0 < n; r0 += chunk) {

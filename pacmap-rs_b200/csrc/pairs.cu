@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_spec_kernel(const flo
 // does. Exact ties always overlap, so they are always settled by the exact distances and the draw order.
 constexpr float MN_REL = 3.0517578125e-05f;  // 2^-15
 template <int E>  // elements per lane of the screening (d = 8 E)
-__global__ void __launch_bounds__(MS_WARPS * 32) sample_mn_screen_kernel(
+__global__ void __launch_bounds__(MS_WARPS * 32, 3) sample_mn_screen_kernel(
     const float* __restrict__ x, const __half* __restrict__ h, const float* __restrict__ eps, uint64_t n, int d,
     uint32_t n_mn, uint64_t seed, uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
   __shared__ uint32_t s_cand[MS_WARPS][MS_MAXC];
