@@ -331,7 +331,9 @@ void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const 
   tm.stop(ST_INIT);
   Csr csr;
   tm.start(ST_CSR);
-  build_csr(c, n, pairs.nn.get(), pairs.n_nn, pairs.mn.get(), pairs.n_mn, pairs.fp.get(), pairs.n_fp, csr);
+  // generated lists come out grouped by point (no device check needed); provided ones are checked
+  build_csr(c, n, pairs.nn.get(), pairs.n_nn, pairs.mn.get(), pairs.n_mn, pairs.fp.get(), pairs.n_fp, csr,
+            cfg.pair_kind == PACMAP_PAIRS_GENERATE);
   tm.stop(ST_CSR);
   DevBuf<float> m(c, n * dim), v(c, n * dim);
   PM_CUDA(cudaMemsetAsync(m.get(), 0, n * dim * sizeof(float), c.stream));

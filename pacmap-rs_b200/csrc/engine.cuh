@@ -100,8 +100,10 @@ struct Csr {
   DevBuf<uint32_t> col;      // partner of each entry, ascending within a segment
   uint64_t entries = 0;
 };
+// grouped_known: the lists are known to hold each point's pairs together (generated lists), so the
+// device check of that (a kernel and a host round trip) is skipped.
 void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const uint32_t* d_pmn, uint64_t n_mn,
-               const uint32_t* d_pfp, uint64_t n_fp, Csr& out);
+               const uint32_t* d_pfp, uint64_t n_fp, Csr& out, bool grouped_known = false);
 void init_value_device(Ctx& c, const float* d_v, uint64_t n, uint64_t dim, float* d_y);
 
 // Every row divided by its norm (the reference's f32 distance from the origin, distance.rs:50-75 order);

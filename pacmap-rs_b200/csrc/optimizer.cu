@@ -532,7 +532,7 @@ Sched schedule_at(uint64_t itr, uint64_t p1, uint64_t p2, float lr) {
 }  // namespace
 
 void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const uint32_t* d_pmn, uint64_t n_mn,
-               const uint32_t* d_pfp, uint64_t n_fp, Csr& out) {
+               const uint32_t* d_pfp, uint64_t n_fp, Csr& out, bool grouped_known) {
   PM_REQUIRE(n < (1ull << 32), PACMAP_ERR_UNSUPPORTED, "pair indices are u32: n must be < 2^32");
   PM_REQUIRE(2 * (n_nn + n_mn + n_fp) < 0xFFFFFFFFull, PACMAP_ERR_UNSUPPORTED, "more than 2^31 pairs");
   const uint64_t nseg = 3 * n;
@@ -547,7 +547,7 @@ void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const u
   bool grouped = n > 0;
   for (int t = 0; t < 3 && grouped; ++t) grouped = sizes[t] % n == 0 && sizes[t] / n < (1ull << 31);
   DevBuf<uint32_t> flag, fwd;
-  if (grouped) {
+  if (grouped && !grouped_known) {
     flag.alloc(c, 1);
     const uint32_t one = 1u;
     PM_CUDA(cudaMemcpyAsync(flag.get(), &one, sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
