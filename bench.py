@@ -432,6 +432,8 @@ def run_ours(args, rank, world, local_rank):
     sl = stages_learned
     # the kNN filter launch that produced the candidates: distance flops of the (row block, column tile)
     # pairs it computed (2 d per score); with tile pruning only the kept pairs
+    # the DRAM traffic figures were captured on the default workload at its full size only
+    traffic = TRAFFIC if (args.workload == "1m-128" and n == WORKLOADS["1m-128"]["n"]) else {}
     knn_ms = sl.get("knn_filter") or 0.0
     tiles = sl.get("knn_tiles_visited") or 0.0  # the main pass's pairs (the bound pass's are not repeated)
     tiles_bound = sl.get("knn_tiles_bound") or 0.0
@@ -440,7 +442,7 @@ def run_ours(args, rank, world, local_rank):
     knn_tf = knn_flops / (knn_ms * 1e-3) / 1e12 if knn_ms > 0 and tiles > 0 else None
     roof_knn = {"kernel": "knn_filter_kernel (tcgen05 distance GEMM + fused candidate filter)", "bound": "tensor",
                 "achieved": round(knn_tf, 2) if knn_tf else None, "peak": bf16, "unit": "TFLOP/s",
-                "frac": round(knn_tf / bf16, 4) if knn_tf else None, "traffic": TRAFFIC.get("knn_filter_kernel"),
+                "frac": round(knn_tf / bf16, 4) if knn_tf else None, "traffic": traffic.get("knn_filter_kernel"),
                 "peak_source": f"{src} bf16 dense (burst: one launch timed alone)",
                 "algorithmic": ("2*d flops per score over the (256-row block, 128-column tile) pairs this launch "
                                 f"computed: {tiles:.0f}, plus {tiles_bound:.0f} in the bound pass, of the full "
@@ -456,7 +458,7 @@ def run_ours(args, rank, world, local_rank):
     opt_gbs = opt_bytes / (opt_ms * 1e-3) / 1e9 if opt_ms > 0 else None
     roof_opt = {"kernel": "grad_adam_kernel (CSR gradient + Adam, one launch per iteration in a CUDA graph)",
                 "bound": "hbm", "achieved": round(opt_gbs, 1) if opt_gbs else None, "peak": hbm, "unit": "GB/s",
-                "frac": round(opt_gbs / hbm, 4) if opt_gbs else None, "traffic": TRAFFIC.get("grad_adam_kernel"),
+                "frac": round(opt_gbs / hbm, 4) if opt_gbs else None, "traffic": traffic.get("grad_adam_kernel"),
                 "algorithmic": ("8 B per active pair + 28*n*dim B per iteration (k, n_mn, n_fp = %d, %d, %d; mid-near "
                                 "pairs inactive in phase 3)" % _pair_counts(n)),
                 "launch_ms": round(opt_ms / iters, 4) if opt_ms else None,
