@@ -316,6 +316,10 @@ uint64_t pacmap_stage_times(double* out_ms, uint64_t cap);
 /* The CUDA stream (cudaStream_t) on which every call for `device` enqueues its work, so that a caller
  * can time calls with events on the launching stream (no reference analogue); NULL on error. */
 void* pacmap_device_stream(int32_t device);
+/* The device's rate of random 8-byte loads from an L2-resident array, in loads per second (diagnostics,
+ * no reference analogue): the ceiling of the gradient's partner gathers, one such load per CSR entry.
+ * Runs for a few milliseconds. */
+pacmap_status pacmap_gather_rate(int32_t device, double* out_loads_per_s);
 /* Kernel launches issued by this thread since the last call of this function (diagnostics). */
 uint64_t pacmap_take_launch_count(void);
 

@@ -875,6 +875,15 @@ pacmap_status pacmap_init_random(uint64_t n, uint64_t dim, uint64_t seed, int32_
   });
 }
 
+pacmap_status pacmap_gather_rate(int32_t device, double* out_loads_per_s) {
+  return guarded([&] {
+    PM_REQUIRE(out_loads_per_s, PACMAP_ERR_INVALID_ARGUMENT, "NULL output");
+    DeviceLock dl(device);
+    *out_loads_per_s = gather_rate_device(dl.ctx);
+    dl.ctx.check_errors("gather rate");
+  });
+}
+
 pacmap_status pacmap_quality(const float* x, uint64_t n, uint64_t d, const float* y, uint64_t dim,
                              const uint32_t* sample, uint64_t n_sample, uint64_t k, const uint32_t* triplets,
                              uint64_t n_triplets, int32_t device, double* out_preservation,

@@ -142,6 +142,8 @@ void gradient_device(Ctx& c, const Csr& csr, const float* d_y, uint64_t n, uint6
                      float w_fp, float* d_grad, float* h_loss);
 
 // ---- metrics.cu ----
+// Random 8-byte loads per second from an L2-resident 8 MB array (best of 3 timed launches).
+double gather_rate_device(Ctx& c);
 void quality_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, const float* d_y, uint64_t dim,
                     const uint32_t* d_sample, uint64_t n_sample, uint64_t k, const uint32_t* d_trip,
                     uint64_t n_trip, double* h_pres, double* h_trip);

@@ -36,7 +36,57 @@ __global__ void triplet_kernel(const float* __restrict__ xh, int d, const float*
   if ((threadIdx.x & 31) == 0 && good) atomicAdd(ok, good);
 }
 
+// The rate of random 8-byte loads from an L2-resident array (the gradient's partner gathers): every
+// thread draws addresses from a hash chain, 8 loads in flight per step; the sum keeps the loads live.
+__device__ __forceinline__ uint32_t hash_step(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352dU;
+  x ^= x >> 15;
+  x *= 0x846ca68bU;
+  x ^= x >> 16;
+  return x;
+}
+
+__global__ void __launch_bounds__(256) gather_rate_kernel(const float2* __restrict__ y, uint32_t n, int reps,
+                                                          float* __restrict__ sink) {
+  uint32_t s = hash_step(blockIdx.x * blockDim.x + threadIdx.x + 1u);
+  float acc = 0.0f;
+  for (int r = 0; r < reps; ++r) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      s = hash_step(s + static_cast<uint32_t>(u));
+      const float2 v = __ldg(&y[s % n]);
+      acc += v.x * v.y;
+    }
+  }
+  if (acc == 1234.5f) sink[0] = acc;  // never true for the zero array; the compiler cannot know that
+}
+
 }  // namespace
+
+double gather_rate_device(Ctx& c) {
+  constexpr uint32_t n = 1u << 20;  // 8 MB: L2-resident, the size of a 1M-point 2-D embedding
+  constexpr int reps = 64, threads = 256;
+  DevBuf<float2> y(c, n);
+  DevBuf<float> sink(c, 1);
+  PM_CUDA(cudaMemsetAsync(y.get(), 0, n * sizeof(float2), c.stream));
+  const unsigned blocks = static_cast<unsigned>(c.sm_count) * 8u;
+  cudaEvent_t ev[2];
+  for (auto& e : ev) PM_CUDA(cudaEventCreate(&e));
+  float ms = 0.0f, best = 0.0f;
+  for (int rep = 0; rep < 4; ++rep) {  // the first launch warms the array into L2
+    PM_CUDA(cudaEventRecord(ev[0], c.stream));
+    gather_rate_kernel<<<blocks, threads, 0, c.stream>>>(y.get(), n, reps, sink.get());
+    PM_LAUNCHED();
+    PM_CUDA(cudaEventRecord(ev[1], c.stream));
+    PM_CUDA(cudaEventSynchronize(ev[1]));
+    PM_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    if (rep > 0 && (best == 0.0f || ms < best)) best = ms;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  const double loads = static_cast<double>(blocks) * threads * reps * 8.0;
+  return best > 0.0f ? loads / (static_cast<double>(best) * 1e-3) : 0.0;
+}
 
 void quality_device(Ctx& c, const float* d_xp, uint64_t n, uint64_t d, const float* d_y, uint64_t dim,
                     const uint32_t* d_sample, uint64_t n_sample, uint64_t k, const uint32_t* d_trip, uint64_t n_trip,

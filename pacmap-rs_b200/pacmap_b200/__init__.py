@@ -324,6 +324,14 @@ def stage_times() -> dict:
     return {name: float(buf[i]) for i, name in enumerate(STAGES[:k])}
 
 
+def gather_rate(device: int = 0) -> float:
+    """Random 8-byte loads per second from an L2-resident 8 MB array on the device: the ceiling of the
+    gradient's partner gathers (one such load per CSR entry)."""
+    v = C.c_double(0.0)
+    _check(_abi.lib().pacmap_gather_rate(int(device), C.byref(v)))
+    return v.value
+
+
 def last_launch_count() -> int:
     """Kernel launches issued by this thread since the previous call."""
     return int(_abi.lib().pacmap_take_launch_count())

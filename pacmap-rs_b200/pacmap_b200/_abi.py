@@ -80,6 +80,7 @@ _SIGS = {
     "pacmap_transform": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _f32, _f32, _vp, _vp, _vp, _i32, _vp]),
     "pacmap_device_stream": (C.c_void_p, [_i32]),
     "pacmap_take_launch_count": (C.c_uint64, []),
+    "pacmap_gather_rate": (C.c_int, [_i32, C.c_void_p]),
     "pacmap_knn_exact_shard_device": (C.c_int, [_vp, _u64, _u64, _u64, _i32, C.c_uint32, C.c_uint32, _i32, _vp, _vp,
                                                 _vp]),
     "pacmap_debug_stall_knn_loads": (C.c_int, [_i32, _i32]),
