@@ -67,20 +67,27 @@ __global__ void grouped_check_kernel(const uint32_t* __restrict__ pairs, uint64_
   if (!__all_sync(0xFFFFFFFFu, ok) && (threadIdx.x & 31) == 0) *flag = 0u;
 }
 
-// Forward counts of grouped lists: segment (i, type) gets the partners j != i of point i's k pairs.
-__global__ void csr_fwd_count_kernel(const uint32_t* __restrict__ pairs, uint64_t n, uint32_t k, int type,
-                                     uint32_t* __restrict__ fwd, uint32_t* __restrict__ cnt,
-                                     uint32_t* __restrict__ err) {
-  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+// Forward counts of grouped lists: segment (i, type) gets the partners j != i of point i's k pairs. One
+// warp per point, its pairs read in coalesced chunks of 32.
+__global__ void __launch_bounds__(256) csr_fwd_count_kernel(const uint32_t* __restrict__ pairs, uint64_t n,
+                                                            uint32_t k, int type, uint32_t* __restrict__ fwd,
+                                                            uint32_t* __restrict__ cnt, uint32_t* __restrict__ err) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * 8 + (threadIdx.x >> 5);
+  const uint32_t lane = threadIdx.x & 31;
   if (i >= n) return;
   uint32_t c = 0;
-  for (uint32_t q = 0; q < k; ++q) {
+  bool bad = false;
+  for (uint32_t q = lane; q < k; q += 32) {
     const uint32_t j = pairs[2 * (i * k + q) + 1];
-    if (j >= n) atomicOr(err, DEV_ERR_PAIR_INDEX);
-    else if (j != i) ++c;
+    bad |= j >= n;
+    c += (j < n && j != i) ? 1u : 0u;
   }
-  fwd[i * 3 + type] = c;
-  cnt[i * 3 + type] = c;
+  c = __reduce_add_sync(0xFFFFFFFFu, c);
+  if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(err, DEV_ERR_PAIR_INDEX);
+  if (lane == 0) {
+    fwd[i * 3 + type] = c;
+    cnt[i * 3 + type] = c;
+  }
 }
 
 __global__ void csr_rev_count_kernel(const uint32_t* __restrict__ pairs, uint64_t P, int type, uint64_t n,
@@ -92,14 +99,21 @@ __global__ void csr_rev_count_kernel(const uint32_t* __restrict__ pairs, uint64_
   }
 }
 
-__global__ void csr_fwd_fill_kernel(const uint32_t* __restrict__ pairs, uint64_t n, uint32_t k, int type,
-                                    const uint32_t* __restrict__ rp, uint32_t* __restrict__ col) {
-  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+// The forward entries of point i's segment in pair order, one warp per point (coalesced reads and writes).
+__global__ void __launch_bounds__(256) csr_fwd_fill_kernel(const uint32_t* __restrict__ pairs, uint64_t n,
+                                                           uint32_t k, int type, const uint32_t* __restrict__ rp,
+                                                           uint32_t* __restrict__ col) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * 8 + (threadIdx.x >> 5);
+  const uint32_t lane = threadIdx.x & 31;
   if (i >= n) return;
   uint32_t pos = rp[i * 3 + type];
-  for (uint32_t q = 0; q < k; ++q) {
-    const uint32_t j = pairs[2 * (i * k + q) + 1];
-    if (j < n && j != i) col[pos++] = j;
+  for (uint32_t q0 = 0; q0 < k; q0 += 32) {
+    const uint32_t q = q0 + lane;
+    const uint32_t j = q < k ? pairs[2 * (i * k + q) + 1] : 0xFFFFFFFFu;
+    const bool keep = q < k && j < n && j != i;
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
+    if (keep) col[pos + __popc(bal & ((1u << lane) - 1u))] = j;
+    pos += __popc(bal);
   }
 }
 
@@ -567,8 +581,8 @@ void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const u
     PM_CUDA(cudaMemsetAsync(fwd.get(), 0, nseg * sizeof(uint32_t), c.stream));
     for (int t = 0; t < 3; ++t) {
       if (!sizes[t]) continue;
-      csr_fwd_count_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(lists[t], n, static_cast<uint32_t>(sizes[t] / n), t,
-                                                                  fwd.get(), cnt.get(), c.d_err);
+      csr_fwd_count_kernel<<<ceil_div(n, 8), 256, 0, c.stream>>>(lists[t], n, static_cast<uint32_t>(sizes[t] / n), t,
+                                                                fwd.get(), cnt.get(), c.d_err);
       PM_LAUNCHED();
     }
     for (int t = 0; t < 3; ++t) {
@@ -603,8 +617,8 @@ void build_csr(Ctx& c, uint64_t n, const uint32_t* d_pnn, uint64_t n_nn, const u
     // forward entries in pair order; reverse entries after them by atomics (cursor = row_ptr + forward)
     for (int t = 0; t < 3; ++t) {
       if (!sizes[t]) continue;
-      csr_fwd_fill_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(lists[t], n, static_cast<uint32_t>(sizes[t] / n), t,
-                                                                 out.row_ptr.get(), out.col.get());
+      csr_fwd_fill_kernel<<<ceil_div(n, 8), 256, 0, c.stream>>>(lists[t], n, static_cast<uint32_t>(sizes[t] / n), t,
+                                                               out.row_ptr.get(), out.col.get());
       PM_LAUNCHED();
     }
     add_offsets_kernel<<<ceil_div(nseg, 256), 256, 0, c.stream>>>(out.row_ptr.get(), fwd.get(), nseg, cnt.get());
