@@ -53,6 +53,8 @@ __global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __res
   __syncthreads();
 
   const int nc8 = (d / 8) * 8;  // the lane-accumulated part; the tail d % 8 is added after the lane sum
+  // rows staged in 16-byte pieces when every row starts on a 16-byte boundary
+  const bool vec4 = (d % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15u) == 0);
   // keys [kbeg, kend) of this block's slice (slice is a multiple of SQ_KT)
   const uint64_t kbeg = static_cast<uint64_t>(blockIdx.y) * slice;
   const uint64_t kend = kbeg + slice < n ? kbeg + slice : n;
@@ -66,15 +68,36 @@ __global__ void __launch_bounds__(SQ_THREADS) knn_simt_kernel(const float* __res
     for (int dbase = 0; dbase < nc8; dbase += SQ_DC) {
       const int dlen = min(SQ_DC, nc8 - dbase);
       __syncthreads();
-      for (int e = tid; e < SQ_QB * dlen; e += SQ_THREADS) {
-        const int qi = e / dlen, cc = e - qi * dlen;
-        const uint64_t r = qrow[qi];
-        qs[qi * SQ_LD + cc] = (r != ~0ull) ? x[r * d + dbase + cc] : 0.0f;
-      }
-      for (int e = tid; e < SQ_KT * dlen; e += SQ_THREADS) {
-        const int kk = e / dlen, cc = e - kk * dlen;
-        const uint64_t j = key0 + kk;
-        ks[kk * SQ_LD + cc] = (j < kend) ? x[j * d + dbase + cc] : 0.0f;
+      if (vec4) {
+        // 16-byte pieces, SQ_DC / 4 per row slot (pieces beyond this pass's dlen are skipped)
+        const int q4 = dlen >> 2;
+        for (int e = tid; e < SQ_QB * (SQ_DC / 4); e += SQ_THREADS) {
+          const int qi = e / (SQ_DC / 4), c4 = e % (SQ_DC / 4);
+          if (c4 >= q4) continue;
+          const uint64_t r = qrow[qi];
+          const float4 v = (r != ~0ull) ? *reinterpret_cast<const float4*>(x + r * d + dbase + 4 * c4)
+                                        : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          *reinterpret_cast<float4*>(&qs[qi * SQ_LD + 4 * c4]) = v;
+        }
+        for (int e = tid; e < SQ_KT * (SQ_DC / 4); e += SQ_THREADS) {
+          const int kk = e / (SQ_DC / 4), c4 = e % (SQ_DC / 4);
+          if (c4 >= q4) continue;
+          const uint64_t j = key0 + kk;
+          const float4 v = (j < kend) ? *reinterpret_cast<const float4*>(x + j * d + dbase + 4 * c4)
+                                      : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          *reinterpret_cast<float4*>(&ks[kk * SQ_LD + 4 * c4]) = v;
+        }
+      } else {
+        for (int e = tid; e < SQ_QB * dlen; e += SQ_THREADS) {
+          const int qi = e / dlen, cc = e - qi * dlen;
+          const uint64_t r = qrow[qi];
+          qs[qi * SQ_LD + cc] = (r != ~0ull) ? x[r * d + dbase + cc] : 0.0f;
+        }
+        for (int e = tid; e < SQ_KT * dlen; e += SQ_THREADS) {
+          const int kk = e / dlen, cc = e - kk * dlen;
+          const uint64_t j = key0 + kk;
+          ks[kk * SQ_LD + cc] = (j < kend) ? x[j * d + dbase + cc] : 0.0f;
+        }
       }
       __syncthreads();
       for (int c8 = 0; c8 < dlen; c8 += 8) {

@@ -194,6 +194,17 @@ __device__ __forceinline__ int compact_row(uint2* __restrict__ cand, int m, int 
   return out;
 }
 
+// The exact band of a buffer that a gather-free (superset) compaction left too full: reloaded and compacted
+// again with every entry's v. Kept out of line: it runs only on hard rows, and the filter's hot loop stays
+// small.
+template <int PER>
+__device__ __noinline__ int recompact_exact(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
+                                            const float2* __restrict__ ge, float& theta_out) {
+  RowRegs<PER> r;
+  load_row<PER>(cand, m, r);
+  return compact_row<PER>(cand, m, min(rank, m), n_i, e4_i, r, 0.0f, ge, theta_out, nullptr, FILTER_SLACK);
+}
+
 // Keeps entries with v <= theta, preserving order; returns the new count. One warp.
 __device__ __forceinline__ int warp_compact(uint32_t* __restrict__ idx, float* __restrict__ v, float* __restrict__ u,
                                             int m, float theta) {
@@ -811,8 +822,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
           const float nL = __shfl_sync(0xFFFFFFFFu, n_i, L);
           const float eL = __shfl_sync(0xFFFFFFFFu, e4_i, L);
           float th;
-          const int kept = compact_row<PER>(cand + rb, m, min(rank, m), nL, eL, cur, e4max, nullptr, th, nullptr,
-                                            FILTER_SLACK);
+          // the gather-free superset first; only when it would not fit, the exact band (the superset holds it,
+          // and its rank smallest upper bounds are those of the whole buffer)
+          int kept = compact_row<PER>(cand + rb, m, min(rank, m), nL, eL, cur, e4max, nullptr, th, nullptr,
+                                      FILTER_SLACK);
+          if (kept > C - TC_BN) kept = recompact_exact<PER>(cand + rb, kept, rank, nL, eL, ge, th);
           if (lane == L) {
             theta = th;
             cnt = kept;
