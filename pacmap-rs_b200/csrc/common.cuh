@@ -233,6 +233,42 @@ __device__ __forceinline__ uint64_t f32x2_fma(uint64_t a, uint64_t b, uint64_t c
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
+// Ascending bitonic sort of 32 R 32-bit keys held in registers by one warp: element r * 32 + lane is
+// v[r] of that lane. Partners closer than 32 elements are exchanged by shuffles, farther ones are registers
+// of the same lane; no shared memory. Every lane must call it (warp-uniform R).
+template <int R>
+__device__ __forceinline__ void warp_sort_regs_u32(uint32_t (&v)[R]) {
+  const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+  for (int size = 2; size <= 32 * R; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {
+        const int rs = stride >> 5;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (r & rs) continue;
+          const uint32_t e = static_cast<uint32_t>(r) * 32u + lane;
+          const bool up = (e & static_cast<uint32_t>(size)) == 0u;
+          const uint32_t a = v[r], b = v[r | rs];
+          const bool sw = (a > b) == up;
+          v[r] = sw ? b : a;
+          v[r | rs] = sw ? a : b;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const uint32_t e = static_cast<uint32_t>(r) * 32u + lane;
+          const uint32_t o = __shfl_xor_sync(0xFFFFFFFFu, v[r], stride);
+          const bool up = (e & static_cast<uint32_t>(size)) == 0u;
+          const bool lower = (lane & static_cast<uint32_t>(stride)) == 0u;
+          v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
+        }
+      }
+    }
+  }
+}
+
 // In-place ascending bitonic sort of `len` (power of two) 64-bit keys in shared memory by one warp.
 __device__ __forceinline__ void warp_bitonic_sort_u64(uint64_t* s, int len) {
   const int lane = threadIdx.x & 31;

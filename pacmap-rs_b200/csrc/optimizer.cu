@@ -18,6 +18,7 @@
 //    snapshot copies as memcpy nodes); the per-iteration (w_nn, w_mn, w_fp, lr_t) schedule lives in a
 //    device table computed with the reference's f32 formulas.
 #include <cmath>
+#include <type_traits>
 #include <cstring>
 #include <string>
 
@@ -247,6 +248,27 @@ __global__ void __launch_bounds__(SEG_WARPS * 32) seg_sort_small_kernel(const ui
     if (len <= 1) continue;
     if (len > SEG_SMALL) {
       if (lane == 0) big[atomicAdd(nbig, 1u)] = static_cast<uint32_t>(sidx);
+      continue;
+    }
+    if (len <= 128) {  // in registers: up to 4 keys per lane
+      auto sort_regs = [&](auto tag) {
+        constexpr int R = decltype(tag)::value;
+        uint32_t v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int t = r * 32 + lane;
+          v[r] = t < len ? col[b + t] : 0xFFFFFFFFu;
+        }
+        warp_sort_regs_u32<R>(v);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int t = r * 32 + lane;
+          if (t < len) col[b + t] = v[r];
+        }
+      };
+      if (len <= 32) sort_regs(std::integral_constant<int, 1>());
+      else if (len <= 64) sort_regs(std::integral_constant<int, 2>());
+      else sort_regs(std::integral_constant<int, 4>());
       continue;
     }
     const int P = next_pow2(len);
