@@ -269,6 +269,41 @@ __device__ __forceinline__ void warp_sort_regs_u32(uint32_t (&v)[R]) {
   }
 }
 
+// The same network for 32 R 64-bit keys in registers.
+template <int R>
+__device__ __forceinline__ void warp_sort_regs_u64(uint64_t (&v)[R]) {
+  const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+  for (int size = 2; size <= 32 * R; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {
+        const int rs = stride >> 5;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (r & rs) continue;
+          const uint32_t e = static_cast<uint32_t>(r) * 32u + lane;
+          const bool up = (e & static_cast<uint32_t>(size)) == 0u;
+          const uint64_t a = v[r], b = v[r | rs];
+          const bool sw = (a > b) == up;
+          v[r] = sw ? b : a;
+          v[r | rs] = sw ? a : b;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const uint32_t e = static_cast<uint32_t>(r) * 32u + lane;
+          const uint64_t o = __shfl_xor_sync(0xFFFFFFFFu, v[r], stride);
+          const bool up = (e & static_cast<uint32_t>(size)) == 0u;
+          const bool lower = (lane & static_cast<uint32_t>(stride)) == 0u;
+          const bool take_min = lower == up;
+          v[r] = ((o < v[r]) == take_min) ? o : v[r];
+        }
+      }
+    }
+  }
+}
+
 // In-place ascending bitonic sort of `len` (power of two) 64-bit keys in shared memory by one warp.
 __device__ __forceinline__ void warp_bitonic_sort_u64(uint64_t* s, int len) {
   const int lane = threadIdx.x & 31;

@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "knn_layout.cuh"
@@ -1015,6 +1016,31 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
     __syncwarp();
     if (nk < K) {  // fewer certified candidates than neighbours (non-finite data): exact fallback
       if (lane == 0) fallback_rows[atomicAdd(n_fallback, 1u)] = static_cast<uint32_t>(orow);
+      __syncwarp();
+      continue;
+    }
+    if (nk <= 128) {  // sorted in registers: up to 4 keys per lane
+      auto sort_regs = [&](auto tag) {
+        constexpr int R = decltype(tag)::value;
+        uint64_t v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int e = r * 32 + lane;
+          v[r] = e < nk ? keys[e] : ~0ull;
+        }
+        warp_sort_regs_u64<R>(v);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int c = r * 32 + lane;
+          if (c < K) {
+            out_idx[orow * K + c] = static_cast<uint32_t>(v[r] & 0xFFFFFFFFu);
+            out_dist[orow * K + c] = key_to_float(static_cast<uint32_t>(v[r] >> 32));
+          }
+        }
+      };
+      if (nk <= 32) sort_regs(std::integral_constant<int, 1>());
+      else if (nk <= 64) sort_regs(std::integral_constant<int, 2>());
+      else sort_regs(std::integral_constant<int, 4>());
       __syncwarp();
       continue;
     }

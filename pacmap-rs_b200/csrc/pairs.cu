@@ -17,6 +17,8 @@
 // registers. Both variants consume the same words in the same order: the pairs are identical.
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 #include "engine.cuh"
 
 namespace pacmap {
@@ -49,15 +51,35 @@ __global__ void __launch_bounds__(RS_WARPS * 32) reselect_kernel(const uint32_t*
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * RS_WARPS + warp; i < n;
        i += static_cast<uint64_t>(gridDim.x) * RS_WARPS) {
     const float si = sig[i];
-    for (int cc = lane; cc < P; cc += 32) {
-      uint64_t key = ~0ull;
-      if (cc < kp) {
-        const float dd = kd[i * kp + cc];
-        const float s = __fdiv_rn(__fmul_rn(dd, dd), __fmul_rn(si, sig[nbr[i * kp + cc]]));
-        key = (static_cast<uint64_t>(total_key(s)) << 32) | static_cast<uint32_t>(cc);
-      }
-      buf[cc] = key;
+    auto key_of = [&](int cc) -> uint64_t {
+      if (cc >= kp) return ~0ull;
+      const float dd = kd[i * kp + cc];
+      const float s = __fdiv_rn(__fmul_rn(dd, dd), __fmul_rn(si, sig[nbr[i * kp + cc]]));
+      return (static_cast<uint64_t>(total_key(s)) << 32) | static_cast<uint32_t>(cc);
+    };
+    if (P <= 128) {  // in registers: up to 4 keys per lane
+      auto sort_regs = [&](auto tag) {
+        constexpr int R = decltype(tag)::value;
+        uint64_t v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = key_of(r * 32 + lane);
+        warp_sort_regs_u64<R>(v);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = r * 32 + lane;
+          if (j < k) {
+            const uint32_t cc = static_cast<uint32_t>(v[r] & 0xFFFFFFFFu);
+            pnn[(i * k + j) * 2 + 0] = static_cast<uint32_t>(i);
+            pnn[(i * k + j) * 2 + 1] = nbr[i * kp + cc];
+          }
+        }
+      };
+      if (P <= 32) sort_regs(std::integral_constant<int, 1>());
+      else if (P <= 64) sort_regs(std::integral_constant<int, 2>());
+      else sort_regs(std::integral_constant<int, 4>());
+      continue;
     }
+    for (int cc = lane; cc < P; cc += 32) buf[cc] = key_of(cc);
     warp_bitonic_sort_u64(buf, P);
     for (int j = lane; j < k; j += 32) {
       const uint32_t cc = static_cast<uint32_t>(buf[j] & 0xFFFFFFFFu);
