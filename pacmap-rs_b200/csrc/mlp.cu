@@ -26,7 +26,7 @@ namespace {
 
 constexpr int MLP_H = 512;
 constexpr int GEMM_THREADS = 192;  // warp 0 TMA, warp 1 MMA + TMEM owner, warps 2..5 epilogue
-constexpr int GEMM_STAGES = 4;
+constexpr int GEMM_STAGES = 2;  // 66 KB at BN = 128: three blocks per SM overlap each other's epilogues
 constexpr int A_STAGE = 128 * 128;  // 128 rows x 64 bf16
 
 enum Epi : int { EPI_F32 = 0, EPI_BIAS_RELU = 1, EPI_DRELU = 2 };
