@@ -756,6 +756,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     const float e4max = __uint_as_float(*e4max_bits);
     bool ok = true;
     uint32_t n_ins = 0, n_comp = 0;  // this row's insertions and compactions (statistics)
+    const int cnt0 = cnt;            // entries carried over from an earlier pass
     auto screen = [&](const uint32_t (&r)[32], int colb) {
       float m8[4];
 #pragma unroll
@@ -764,18 +765,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
         m8[g] = fmax3(fmax3(D[0], D[1], D[2]), fmax3(D[3], D[4], D[5]), fmaxf(D[6], D[7]));
       }
       const float m = fmaxf(fmax3(m8[0], m8[1], m8[2]), m8[3]);
-      if (__any_sync(0xFFFFFFFFu, -2.0f * m <= theta)) {
+      // v = -2 D <= theta exactly when D >= -theta / 2 (both scalings by 2 are exact)
+      const float hth = -0.5f * theta;
+      if (__any_sync(0xFFFFFFFFu, m >= hth)) {
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
-          if (__any_sync(0xFFFFFFFFu, -2.0f * m8[g] <= theta)) {
+          if (__any_sync(0xFFFFFFFFu, m8[g] >= hth)) {
 #pragma unroll
             for (int c = 8 * g; c < 8 * g + 8; ++c) {
-              const float v = -2.0f * __uint_as_float(r[c]);
-              if (v <= theta) {
+              const float D = __uint_as_float(r[c]);
+              if (D >= hth) {
                 const uint32_t col = static_cast<uint32_t>(colb + c);
-                cand[cbase + cnt] = make_uint2(col, __float_as_uint(v + __ldg(&ge[col].y)));
+                cand[cbase + cnt] = make_uint2(col, __float_as_uint(-2.0f * D + __ldg(&ge[col].y)));
                 ++cnt;
-                ++n_ins;
               }
             }
           }
@@ -837,6 +839,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
               cnt = 0;
               overflow_rows[atomicAdd(n_overflow, 1u)] = perm[row];
             }
+            n_ins += static_cast<uint32_t>(m - cnt);  // the entries this compaction dropped
           }
           __syncwarp();
           if (L2 < 0) break;
@@ -852,6 +855,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
       sh->abort_flag = 1;
     }
     if (valid) cand_cnt[row] = (theta == -__int_as_float(0x7f800000)) ? -1 : cnt;
+    n_ins += static_cast<uint32_t>(cnt - cnt0);  // dropped + left = inserted + present at the start
     if (counters) {
       const uint32_t wi = __reduce_add_sync(0xFFFFFFFFu, n_ins), wc = __reduce_add_sync(0xFFFFFFFFu, n_comp);
       if (lane == 0) {
