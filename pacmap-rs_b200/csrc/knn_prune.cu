@@ -55,31 +55,49 @@ __global__ void __launch_bounds__(256) pivot_dmin_kernel(const float* __restrict
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int PER_WARP = PV_CHUNK / 8;
   double ws = 0.0;
-  for (int t = 0; t < PER_WARP; ++t) {
-    const uint32_t s = blockIdx.x * PV_CHUNK + warp * PER_WARP + t;
-    if (s >= S) break;  // warp-uniform
-    const float* xr = x + sub_row(s, S, n) * d;
-    float acc[PV_BATCH];
+  // four subsample rows at a time (their loads in flight together); each row's sums and the order of
+  // the block's double sum are those of one row at a time
+  static_assert(PER_WARP % 4 == 0, "rows are taken four at a time");
+  for (int t0 = 0; t0 < PER_WARP; t0 += 4) {
+    const uint32_t s0 = blockIdx.x * PV_CHUNK + warp * PER_WARP + t0;
+    if (s0 >= S) break;  // warp-uniform
+    const float* xr[4];
 #pragma unroll
-    for (int q = 0; q < PV_BATCH; ++q) acc[q] = 0.0f;
+    for (int u = 0; u < 4; ++u) xr[u] = x + sub_row(s0 + u < S ? s0 + u : s0, S, n) * d;
+    float acc[4][PV_BATCH];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int q = 0; q < PV_BATCH; ++q) acc[u][q] = 0.0f;
     for (int col = lane; col < d; col += 32) {
-      const float xv = xr[col];
+      float xv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) xv[u] = xr[u][col];
 #pragma unroll
       for (int q = 0; q < PV_BATCH; ++q) {
-        const float df = xv - pv[q * d + col];
-        acc[q] = fmaf(df, df, acc[q]);
+        const float pq = pv[q * d + col];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float df = xv[u] - pq;
+          acc[u][q] = fmaf(df, df, acc[u][q]);
+        }
       }
     }
-    float best = p0 == 0 ? __int_as_float(0x7f800000) : dmin[s];
 #pragma unroll
-    for (int q = 0; q < PV_BATCH; ++q) {
-      float v = acc[q];
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t s = s0 + u;
+      if (s >= S) break;  // warp-uniform
+      float best = p0 == 0 ? __int_as_float(0x7f800000) : dmin[s];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);  // the same sum on every lane
-      best = fminf(best, v);
+      for (int q = 0; q < PV_BATCH; ++q) {
+        float v = acc[u][q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);  // the same sum on every lane
+        best = fminf(best, v);
+      }
+      if (lane == 0) dmin[s] = best;
+      if (best < 3.0e38f) ws += static_cast<double>(best);
     }
-    if (lane == 0) dmin[s] = best;
-    if (best < 3.0e38f) ws += static_cast<double>(best);
   }
   if (lane == 0) wsum[warp] = ws;
   __syncthreads();
@@ -93,22 +111,27 @@ __global__ void __launch_bounds__(256) pivot_dmin_kernel(const float* __restrict
 // Round 0: 16 evenly spaced subsample points. Round r > 0: 16 draws, each point with probability
 // proportional to dmin (its squared distance to the nearest pivot so far); a degenerate subsample (all
 // dmin zero) falls back to evenly spaced points.
-__global__ void __launch_bounds__(64) pivot_draw_kernel(const float* __restrict__ dmin, uint32_t S, uint64_t n,
-                                                        const double* __restrict__ chunk_sum, int nchunks, int round,
-                                                        uint32_t* __restrict__ piv_rows) {
+__global__ void __launch_bounds__(PV_BATCH * 32) pivot_draw_kernel(const float* __restrict__ dmin, uint32_t S,
+                                                                   uint64_t n, const double* __restrict__ chunk_sum,
+                                                                   int nchunks, int round,
+                                                                   uint32_t* __restrict__ piv_rows) {
+  __shared__ double cs[PV_SUB_MAX / PV_CHUNK];
   __shared__ double pre[PV_SUB_MAX / PV_CHUNK + 1];
-  if (threadIdx.x == 0) {
+  for (int ch = threadIdx.x; round > 0 && ch < nchunks; ch += blockDim.x) cs[ch] = chunk_sum[ch];
+  __syncthreads();
+  if (threadIdx.x == 0) {  // the prefix in chunk order, from shared memory
     double run = 0.0;
     pre[0] = 0.0;
     for (int ch = 0; round > 0 && ch < nchunks; ++ch) {
-      const double v = chunk_sum[ch];
+      const double v = cs[ch];
       run += (v > 0.0 && v < 1e300) ? v : 0.0;
       pre[ch + 1] = run;
     }
   }
   __syncthreads();
-  const int b = threadIdx.x;
-  if (b >= PV_BATCH) return;
+  // one warp per draw: the chunk's dmin values read 32 at a time, then added in index order on every lane
+  // (the same sequence of double additions as one thread walking the chunk)
+  const int b = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
   uint32_t s = round == 0 ? static_cast<uint32_t>(static_cast<uint64_t>(b) * S / PV_BATCH)
                           : static_cast<uint32_t>(static_cast<uint64_t>(round * PV_BATCH + b) * S / PIV);
   const double total = round > 0 ? pre[nchunks] : 0.0;
@@ -126,17 +149,22 @@ __global__ void __launch_bounds__(64) pivot_draw_kernel(const float* __restrict_
     double acc = pre[lo];
     const uint32_t a = static_cast<uint32_t>(lo) * PV_CHUNK, e = min(S, a + PV_CHUNK);
     uint32_t pick = 0xFFFFFFFFu;
-    for (uint32_t t = a; t < e; ++t) {
-      const float v = dmin[t];
-      if (v > 0.0f && v < 3.0e38f) {
-        pick = t;
-        acc += v;
-        if (acc > target) break;
+    bool done = false;
+    for (uint32_t base = a; base < e && !done; base += 32) {
+      const uint32_t t = base + static_cast<uint32_t>(lane);
+      const float mine = t < e ? dmin[t] : 0.0f;
+      for (int k = 0; k < 32; ++k) {
+        const float v = __shfl_sync(0xFFFFFFFFu, mine, k);
+        if (!done && base + k < e && v > 0.0f && v < 3.0e38f) {
+          pick = base + static_cast<uint32_t>(k);
+          acc += v;
+          if (acc > target) done = true;
+        }
       }
     }
     if (pick != 0xFFFFFFFFu) s = pick;
   }
-  piv_rows[round * PV_BATCH + b] = static_cast<uint32_t>(sub_row(s, S, n));
+  if (lane == 0) piv_rows[round * PV_BATCH + b] = static_cast<uint32_t>(sub_row(s, S, n));
 }
 
 // Per column tile (128 positions): its rows split by pivot cell into at most SEGS segments (cells are
@@ -462,13 +490,13 @@ void select_pivots(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint32_t* d
   DevBuf<double> csum(c, nchunks);
   const size_t smem = static_cast<size_t>(PV_BATCH) * d * sizeof(float);
   PM_CUDA(cudaFuncSetAttribute(pivot_dmin_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  pivot_draw_kernel<<<1, 64, 0, c.stream>>>(dmin.get(), S, n, csum.get(), nchunks, 0, d_piv_rows);
+  pivot_draw_kernel<<<1, PV_BATCH * 32, 0, c.stream>>>(dmin.get(), S, n, csum.get(), nchunks, 0, d_piv_rows);
   PM_LAUNCHED();
   for (int r = 1; r < PIV / PV_BATCH; ++r) {
     pivot_dmin_kernel<<<nchunks, 256, smem, c.stream>>>(d_x, n, static_cast<int>(d), S, d_piv_rows, (r - 1) * PV_BATCH,
                                                         dmin.get(), csum.get());
     PM_LAUNCHED();
-    pivot_draw_kernel<<<1, 64, 0, c.stream>>>(dmin.get(), S, n, csum.get(), nchunks, r, d_piv_rows);
+    pivot_draw_kernel<<<1, PV_BATCH * 32, 0, c.stream>>>(dmin.get(), S, n, csum.get(), nchunks, r, d_piv_rows);
     PM_LAUNCHED();
   }
 }
