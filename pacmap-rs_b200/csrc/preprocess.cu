@@ -45,6 +45,7 @@ __global__ void minmax_keys_kernel(const float* __restrict__ x, uint64_t total, 
 constexpr int CQ_COLS = 32;    // columns per chain warp (one lane each)
 constexpr int CQ_ROWS = 256;   // rows per TMA tile (32 KB)
 constexpr int CQ_STAGES = 6;
+static_assert(CQ_ROWS % 32 == 0, "the chain's full tiles run in steps of 32 rows");
 
 // y = (x - sub) / div (two separately rounded f32 operations) into Y [n][dp], padding columns 0.
 __global__ void scale_pad_kernel(const float* __restrict__ x, uint64_t n, uint64_t d, uint64_t dp, float sub,
@@ -123,24 +124,27 @@ __global__ void __launch_bounds__(64) colsum_chain_kernel(const __grid_constant_
     }
     const float* b = buf + st * CQ_ROWS * CQ_COLS + lane;
     const int rows = static_cast<int>(n - t * CQ_ROWS < CQ_ROWS ? n - t * CQ_ROWS : CQ_ROWS);
-    int r = 0;
-    if (rows >= 16) {
-      float cur[16];
+    if (rows == CQ_ROWS) {
+      // a full tile: two register sets in turn, one loaded while the other is added (no copies)
+      float A[16], B[16];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) cur[q] = b[q * CQ_COLS];
-      for (r = 16; r + 16 <= rows; r += 16) {
-        float nxt[16];
+      for (int q = 0; q < 16; ++q) A[q] = b[q * CQ_COLS];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) nxt[q] = b[(r + q) * CQ_COLS];
+      for (int r = 0; r < CQ_ROWS; r += 32) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) s = __fadd_rn(s, cur[q]);
+        for (int q = 0; q < 16; ++q) B[q] = b[(r + 16 + q) * CQ_COLS];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) cur[q] = nxt[q];
+        for (int q = 0; q < 16; ++q) s = __fadd_rn(s, A[q]);
+        if (r + 32 < CQ_ROWS) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) A[q] = b[(r + 32 + q) * CQ_COLS];
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) s = __fadd_rn(s, B[q]);
       }
-#pragma unroll
-      for (int q = 0; q < 16; ++q) s = __fadd_rn(s, cur[q]);
+    } else {
+      for (int r = 0; r < rows; ++r) s = __fadd_rn(s, b[r * CQ_COLS]);
     }
-    for (; r < rows; ++r) s = __fadd_rn(s, b[r * CQ_COLS]);
     __syncwarp();
     if (lane == 0) mbar_arrive(&sh->empty[st]);
   }
