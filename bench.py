@@ -458,7 +458,12 @@ def run_ours(args, rank, world, local_rank):
                 "tiles_computed_frac": round((tiles + tiles_bound) / tiles_full, 4) if tiles_full else None,
                 "bound_pass_ms": round(sl.get("knn_bound", 0.0), 3),
                 "exact_knn_stage_ms": round(sl.get("knn", 0.0), 3),
-                "full_square_equivalent_tflops": round(2.0 * n * n * d / (sl["knn"] * 1e-3) / 1e12, 1) if sl.get("knn") else None}
+                "full_square_equivalent_tflops": round(2.0 * n * n * d / (sl["knn"] * 1e-3) / 1e12, 1) if sl.get("knn") else None,
+                "bound_by": ("the epilogue's candidate screening and insertion (per row: %.0f insertions, %.1f "
+                             "compactions, %.0f candidates left for the exact re-rank); the tensor pipe is busy a few "
+                             "per cent of the launch" % (sl.get("knn_insertions_per_row", 0.0),
+                                                         sl.get("knn_compactions_per_row", 0.0),
+                                                         sl.get("knn_band_per_row", 0.0)))}
     opt_ms = sl.get("optimize", 0.0)
     iters = sum(learned.SHORT_SCHEDULE)
     opt_bytes = _optimize_bytes(n, dim, learned.SHORT_SCHEDULE)
