@@ -309,7 +309,8 @@ pacmap_status pacmap_preprocess_noalloc(const float* d_x, uint64_t n, uint64_t d
  * kNN ran: its filter kernel alone, the number of rows it left to the exact fallback, the time of the
  * tile pruning's bound pass and lists, the (row block, column tile) pairs computed, of the full
  * sweep, and of the bound pass, and per row: candidate entries written by the filter passes, compactions
- * inside them, and candidates left for the exact re-rank), and returns how many. */
+ * inside them, and candidates left for the exact re-rank; then the host milliseconds spent capturing and
+ * instantiating the optimiser's CUDA graph, part of the optimize stage), and returns how many. */
 void pacmap_set_stage_timing(int32_t enabled);
 uint64_t pacmap_stage_times(double* out_ms, uint64_t cap);
 

@@ -357,6 +357,10 @@ void fit_transform_impl(Ctx& c, const float* d_x, uint64_t n, uint64_t d, const 
   tm.start(ST_OPT);
   optimize_device(c, csr, a);
   tm.stop(ST_OPT);
+  if (tm.on) {
+    g_stage_ms.resize(std::max<size_t>(g_stage_ms.size(), ST_COUNT + 10), 0.0);
+    g_stage_ms[ST_COUNT + 9] = last_graph_setup_ms();
+  }
   c.check_errors("optimiser");
 }
 

@@ -137,6 +137,8 @@ struct OptimizeArgs {
   float* d_grad_last = nullptr;         // (n+1) x dim gradient of the last iteration, may be NULL
 };
 void optimize_device(Ctx& c, const Csr& csr, const OptimizeArgs& a);
+// Host milliseconds the last optimize_device on this thread spent capturing and instantiating its graph.
+double& last_graph_setup_ms();
 // One gradient evaluation with explicit weights: d_grad (n x dim), *h_loss the loss.
 void gradient_device(Ctx& c, const Csr& csr, const float* d_y, uint64_t n, uint64_t dim, float w_nn, float w_mn,
                      float w_fp, float* d_grad, float* h_loss);

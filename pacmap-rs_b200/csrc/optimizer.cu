@@ -17,10 +17,11 @@
 // K9 optimize_device: all iterations are captured into one CUDA graph (one kernel node per iteration,
 //    snapshot copies as memcpy nodes); the per-iteration (w_nn, w_mn, w_fp, lr_t) schedule lives in a
 //    device table computed with the reference's f32 formulas.
+#include <chrono>
 #include <cmath>
-#include <type_traits>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "engine.cuh"
 
@@ -726,6 +727,11 @@ void init_random_device(Ctx& c, uint64_t n, uint64_t dim, uint64_t seed, float* 
   PM_LAUNCHED();
 }
 
+double& last_graph_setup_ms() {
+  static thread_local double v = 0.0;
+  return v;
+}
+
 void optimize_device(Ctx& c, const Csr& csr, const OptimizeArgs& a) {
   const uint64_t n = a.n, dim = a.dim;
   if (a.itr_end <= a.itr_begin || n == 0 || dim == 0) return;
@@ -755,6 +761,7 @@ void optimize_device(Ctx& c, const Csr& csr, const OptimizeArgs& a) {
 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  const auto setup_t0 = std::chrono::steady_clock::now();
   PM_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
   uint64_t launches = 0;
   bool capture_ok = true;
@@ -788,6 +795,8 @@ void optimize_device(Ctx& c, const Csr& csr, const OptimizeArgs& a) {
     throw Fail{PACMAP_ERR_CUDA, "graph capture failed: " + capture_msg + " " + cudaGetErrorString(end_err)};
   }
   const cudaError_t inst = cudaGraphInstantiate(&exec, graph, 0);
+  last_graph_setup_ms() =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - setup_t0).count();
   if (inst != cudaSuccess) {
     cudaGraphDestroy(graph);
     throw Fail{PACMAP_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(inst)};

@@ -309,7 +309,7 @@ def quality(x, y, sample, triplets, k: int = 10, device: int = 0):
 
 STAGES = ("preprocess", "knn", "reselect", "sample_mn", "sample_fp", "csr", "init", "optimize", "knn_filter",
           "knn_fallback_rows", "knn_bound", "knn_tiles_visited", "knn_tiles_full", "knn_tiles_bound",
-          "knn_insertions_per_row", "knn_compactions_per_row", "knn_band_per_row")
+          "knn_insertions_per_row", "knn_compactions_per_row", "knn_band_per_row", "optimize_graph_setup")
 
 
 def set_stage_timing(enabled: bool) -> None:
