@@ -214,6 +214,36 @@ def test_gradient_matches_oracle(lib, orc):
         assert abs(got[-1, 0] - exp64[-1, 0]) <= 1e-5 * abs(exp64[-1, 0])
 
 
+def _hub_pairs(n, seed):
+    """Grouped pair lists whose far partners are skewed towards hubs, so that CSR segments take every
+    sorting path: most hold < 32 entries, 30 mid hubs ~100 (4 keys per lane in registers), 5 big hubs ~240
+    (shared memory)."""
+    rng = np.random.default_rng(seed)
+    def grouped(k, partners):
+        a = np.repeat(np.arange(n), k)
+        return np.stack([a, partners.reshape(-1)], 1).astype(np.uint32)
+    nn = rng.integers(0, n, size=(n, 10))
+    mn = rng.integers(0, n, size=(n, 5))
+    u = rng.random(size=(n, 20))
+    fp = np.where(u < 0.02, rng.integers(0, 5, size=(n, 20)),
+                  np.where(u < 0.07, 5 + rng.integers(0, 30, size=(n, 20)), rng.integers(0, n, size=(n, 20))))
+    return grouped(10, nn), grouped(5, mn), grouped(20, fp)
+
+
+def test_gradient_with_hub_segments_matches_oracle_and_is_deterministic(lib, orc):
+    n = 3000
+    pnn, pmn, pfp = _hub_pairs(n, 12)
+    y = np.random.default_rng(1).normal(size=(n, 2)).astype(np.float32)
+    w = (2.0, 1000.0, 1.0)
+    got = lib.stages.gradient(y, pnn, pmn, pfp, *w)
+    again = lib.stages.gradient(y, pnn, pmn, pfp, *w)
+    # every segment is sorted, so the summation order (and the result) is the same on every call
+    assert np.array_equal(got, again)
+    exp, exp64, absum = orc.grad(y, pnn, pmn, pfp, *w, with64=True)
+    assert (np.abs(got[:-1] - exp[:-1]) <= GRAD_TOL * absum + 1e-30).all()
+    assert (np.abs(got[:-1] - exp64[:-1]) <= GRAD_TOL * absum + 1e-30).all()
+
+
 @pytest.mark.parametrize("itr", [0, 1, 37, 99, 100, 150, 199, 200, 300, 449])
 def test_each_iteration_matches_oracle(lib, orc, itr):
     """AllProvided pairs + identical state: one GPU iteration vs one oracle iteration."""
