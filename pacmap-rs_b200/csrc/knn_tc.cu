@@ -16,8 +16,10 @@
 //     Each row keeps a buffer of candidates (j, u = v + 4 e_j) with v <= theta_i, where theta_i comes from
 //     the (k'+1)-th smallest UB seen so far (the +1 covers the row itself); when the buffer fills, the
 //     owning warp compacts it (the rank-th smallest u by bisection on warp-wide counts; inside the filter
-//     the kept set is u <= theta + max 4 e, a superset of the band, so no per-entry gather is needed).
-//     Any true neighbour has LB <= k'-th UB, so it is never dropped.
+//     the kept set is u <= theta + max 4 e, a superset of the band, so no per-entry gather is needed,
+//     unless that superset would not fit: then the exact band, with every entry's own e_j).
+//     Any true neighbour has LB <= k'-th UB, so it is never dropped. From 32,768 rows the tile pruning
+//     (knn_prune.cu) restricts each row block to the column tiles that may hold one of its neighbours.
 //  3. knn_rerank_kernel: the final threshold, then the reference's exact f32 distance of every
 //     survivor, sorted by (distance, index): the rows of knn.rs.
 //  Rows whose candidate band does not fit the buffer (e.g. thousands of exact duplicates) are
