@@ -13,11 +13,11 @@
 //     Cauchy-Schwarz bound of h.l + l.h + l.l, eta = tensor-core accumulation, gamma = every f32
 //     rounding incl. the reference's own distance sum), the reference's squared distance lies in
 //     [LB, UB] = [v + n_i - 2e_i, v + 4e_j + n_i + 2e_i].
-//     Each row keeps a buffer of candidates (j, u = v + 4 e_j) with v <= theta_i, where theta_i comes from
-//     the (k'+1)-th smallest UB seen so far (the +1 covers the row itself); when the buffer fills, the
-//     owning warp compacts it (the rank-th smallest u by bisection on warp-wide counts; inside the filter
-//     the kept set is u <= theta + max 4 e, a superset of the band, so no per-entry gather is needed,
-//     unless that superset would not fit: then the exact band, with every entry's own e_j).
+//     Each row keeps a buffer of candidates (j, v) with v <= theta_i, where theta_i comes from the
+//     (k'+1)-th smallest UB seen so far (the +1 covers the row itself); when the buffer fills, the owning
+//     warp compacts it (the rank-th smallest by bisection on warp-wide counts; inside the filter the UB of
+//     an entry is bounded with the largest e, so no per-entry gather is needed, unless the band would not
+//     fit: then again with every entry's own e_j). The final compaction uses every entry's own e_j.
 //     Any true neighbour has LB <= k'-th UB, so it is never dropped. From 32,768 rows the tile pruning
 //     (knn_prune.cu) restricts each row block to the column tiles that may hold one of its neighbours.
 //  3. knn_rerank_kernel: the final threshold, then the reference's exact f32 distance of every
@@ -96,23 +96,24 @@ struct FilterLayout {
 // Per-row candidate buffer maintenance (shared by the filter's compaction and the re-rank).
 // ---------------------------------------------------------------------------------------------
 
-// theta for row constants (n_i, e4_i = 4 e_i) and the selected UB key: v <= theta keeps every
-// candidate whose lower bound is within the (sqrt-tie-widened) k'-th upper bound.
-__device__ __forceinline__ float theta_from(uint32_t ukey, float n_i, float e4_i) {
-  const float uT = key_to_float(ukey);
+// theta for row constants (n_i, e4_i = 4 e_i) and the selected u (UB less n_i + 2 e_i): v <= theta keeps
+// every candidate whose lower bound is within the (sqrt-tie-widened) k'-th upper bound. Non-decreasing in
+// uT, so any uT at or above the rank-th smallest u gives a valid (looser) theta.
+__device__ __forceinline__ float theta_from(float uT, float n_i, float e4_i) {
   const float base = uT + e4_i;
   const float slack = 9.5367431640625e-07f * fabsf(uT + n_i + 0.5f * e4_i) + 2.384185791015625e-07f * (n_i + fabsf(uT));
   return base + slack;
 }
 
-// Candidate entries are (index j, u = v + 4 e_j): u is the upper bound of the reference's squared distance
-// less n_i + 2 e_i, v = u - 4 e_j the lower one less n_i - 2 e_i (both scaled by s^2).
+// Candidate entries are (index j, v = -2 D): v + n_i - 2 e_i is the lower bound of the reference's squared
+// distance and u = fl(v + 4 e_j) + n_i + 2 e_i the upper one (scaled by s^2). v is exact (D scaled by -2),
+// so the insertion needs no per-column constant and every later u is the same f32 value.
 //
 // A row's buffer in registers (m <= 32 * PER entries), loaded once per compaction by the whole warp.
 template <int PER>
 struct RowRegs {
   uint32_t ri[PER];
-  float ru[PER];
+  float rv[PER];
 };
 template <int PER>
 __device__ __forceinline__ void load_row(const uint2* __restrict__ cand, int m, RowRegs<PER>& r) {
@@ -122,29 +123,34 @@ __device__ __forceinline__ void load_row(const uint2* __restrict__ cand, int m, 
     const int e = q * 32 + lane;
     const uint2 cv = e < m ? cand[e] : make_uint2(0u, 0u);
     r.ri[q] = cv.x;
-    r.ru[q] = __uint_as_float(cv.y);
+    r.rv[q] = __uint_as_float(cv.y);
   }
 }
 
-// Compaction of one row's buffer from its registers, one warp: the rank-`rank` smallest u by bisection
-// on warp-wide counts, theta from it, and the entries of the row's certified band (v <= theta) written
-// back in order. With ge (the separate compaction kernels) v = u - 4 e_j is recovered exactly up to one
-// rounding (kept when within 2^-22 of the magnitudes above theta); without it (inside the filter, where
-// a gather per entry would stall the epilogue) an entry is kept when u <= theta + e4max, a superset.
-// slack > 0 ends the bisection at the first key T with rank <= #{keys <= T} <= rank + slack: T is then
-// at or above the rank-th smallest key, so theta still bounds the row's k'-th neighbour (a looser bound
-// for fewer serial steps; the filter's compactions use it, the final one is exact).
+// Compaction of one row's buffer from its registers, one warp: the rank-`rank` smallest u by bisection on
+// warp-wide counts, theta from it, and the row's band (v <= theta) written back in order. With ge (the
+// separate compaction kernel, and the filter's second compaction) u_j = fl(v_j + 4 e_j) with each entry's
+// own e_j. Without it (inside the filter, where a gather per entry would stall the epilogue) the keys are v
+// and the rank-th smallest u is bounded by fl(vT + e4max) for the rank-th smallest v = vT (rounding is
+// monotone and e4_j <= e4max), a looser but valid theta. theta is capped by theta_cap, an earlier valid
+// threshold of the same row (every theta is at or above the row's final one, so the band keeps every
+// neighbour; the entries that defined the smaller of the two all pass it, so at least `rank` are kept).
+// slack > 0 ends the bisection at the first key T with rank <= #{keys <= T} <= rank + slack: T is then at or
+// above the rank-th smallest key (a looser bound for fewer serial steps; the final compaction is exact).
 template <int PER>
 __device__ __forceinline__ int compact_row(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
                                            const RowRegs<PER>& r, float e4max, const float2* __restrict__ ge,
-                                           float& theta_out, uint32_t* ukey_out = nullptr, int slack = 0) {
+                                           float theta_cap, float& theta_out, uint32_t* ukey_out = nullptr,
+                                           int slack = 0) {
   const int lane = threadIdx.x & 31;
   uint32_t rk[PER];
   uint32_t kmin = 0xFFFFFFFFu, kmax = 0u;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
     const bool in = q * 32 + lane < m;
-    rk[q] = in ? total_key(r.ru[q]) : 0xFFFFFFFFu;
+    float key = r.rv[q];
+    if (ge) key = __fadd_rn(key, in ? __ldg(&ge[r.ri[q]].y) : 0.0f);
+    rk[q] = in ? total_key(key) : 0xFFFFFFFFu;
     if (in) {
       kmin = min(kmin, rk[q]);
       kmax = max(kmax, rk[q]);
@@ -168,26 +174,16 @@ __device__ __forceinline__ int compact_row(uint2* __restrict__ cand, int m, int 
     }
   }
   const uint32_t prefix = hi;
-  const float th = theta_from(prefix, n_i, e4_i);
-  float e4j[PER];
-  if (ge) {
-#pragma unroll
-    for (int q = 0; q < PER; ++q) e4j[q] = q * 32 + lane < m ? __ldg(&ge[r.ri[q]].y) : 0.0f;
-  }
+  const float uT = ge ? key_to_float(prefix) : __fadd_rn(key_to_float(prefix), e4max);
+  const float th = fminf(theta_from(uT, n_i, e4_i), theta_cap);
   int out = 0;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
-    bool keep = q * 32 + lane < m;
-    if (ge) {
-      const float v = r.ru[q] - e4j[q];
-      keep = keep && v <= th + 2.384185791015625e-07f * (fabsf(r.ru[q]) + e4j[q]);
-    } else {
-      keep = keep && r.ru[q] <= (th + e4max) + 2.384185791015625e-07f * (fabsf(th) + e4max);
-    }
+    const bool keep = q * 32 + lane < m && r.rv[q] <= th;
     const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
     if (keep) {
       const int pos = out + __popc(bal & ((1u << lane) - 1u));
-      cand[pos] = make_uint2(r.ri[q], __float_as_uint(r.ru[q]));
+      cand[pos] = make_uint2(r.ri[q], __float_as_uint(r.rv[q]));
     }
     out += __popc(bal);
   }
@@ -197,47 +193,16 @@ __device__ __forceinline__ int compact_row(uint2* __restrict__ cand, int m, int 
   return out;
 }
 
-// The exact band of a buffer that a gather-free (superset) compaction left too full: reloaded and compacted
-// again with every entry's v. Kept out of line: it runs only on hard rows, and the filter's hot loop stays
+// The band of a buffer that the gather-free compaction left too full, compacted again with every entry's
+// own e_j (a tighter theta). Kept out of line: it runs only on hard rows, and the filter's hot loop stays
 // small.
 template <int PER>
 __device__ __noinline__ int recompact_exact(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
-                                            const float2* __restrict__ ge, float& theta_out) {
+                                            const float2* __restrict__ ge, float theta_cap, float& theta_out) {
   RowRegs<PER> r;
   load_row<PER>(cand, m, r);
-  return compact_row<PER>(cand, m, min(rank, m), n_i, e4_i, r, 0.0f, ge, theta_out, nullptr, FILTER_SLACK);
-}
-
-// Keeps entries with v <= theta, preserving order; returns the new count. One warp.
-__device__ __forceinline__ int warp_compact(uint32_t* __restrict__ idx, float* __restrict__ v, float* __restrict__ u,
-                                            int m, float theta) {
-  const int lane = threadIdx.x & 31;
-  int out = 0;
-  for (int e0 = 0; e0 < m; e0 += 32) {
-    const int e = e0 + lane;
-    uint32_t ii = 0;
-    float vv = 0.0f, uu = 0.0f;
-    bool keep = false;
-    if (e < m) {
-      vv = v[e];
-      keep = vv <= theta;
-      if (keep) {
-        ii = idx[e];
-        uu = u[e];
-      }
-    }
-    const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
-    __syncwarp();
-    if (keep) {
-      const int pos = out + __popc(bal & ((1u << lane) - 1u));
-      idx[pos] = ii;
-      v[pos] = vv;
-      u[pos] = uu;
-    }
-    out += __popc(bal);
-    __syncwarp();
-  }
-  return out;
+  return compact_row<PER>(cand, m, min(rank, m), n_i, e4_i, r, 0.0f, ge, theta_cap, theta_out, nullptr,
+                          FILTER_SLACK);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -773,14 +738,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
           if (__any_sync(0xFFFFFFFFu, m8[g] >= hth)) {
+            // every column of the group without a branch: a predicated store of (j, v = -2 D) and a
+            // predicated count (a divergent branch per column cost more than the column's work)
 #pragma unroll
             for (int c = 8 * g; c < 8 * g + 8; ++c) {
               const float D = __uint_as_float(r[c]);
-              if (D >= hth) {
-                const uint32_t col = static_cast<uint32_t>(colb + c);
-                cand[cbase + cnt] = make_uint2(col, __float_as_uint(-2.0f * D + __ldg(&ge[col].y)));
-                ++cnt;
-              }
+              st_global_v2_if_ge(cand + cbase + cnt, static_cast<uint32_t>(colb + c), __float_as_uint(-2.0f * D), D,
+                                 hth);
+              cnt += D >= hth ? 1 : 0;
             }
           }
         }
@@ -827,11 +792,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
           const float nL = __shfl_sync(0xFFFFFFFFu, n_i, L);
           const float eL = __shfl_sync(0xFFFFFFFFu, e4_i, L);
           float th;
-          // the gather-free superset first; only when it would not fit, the exact band (the superset holds it,
-          // and its rank smallest upper bounds are those of the whole buffer)
-          int kept = compact_row<PER>(cand + rb, m, min(rank, m), nL, eL, cur, e4max, nullptr, th, nullptr,
+          // gather-free first (theta from the largest e); only when its band would not fit, again with every
+          // entry's own e_j (the band holds the rank entries of smallest u, so the tighter theta is the
+          // whole buffer's)
+          const float thL = __shfl_sync(0xFFFFFFFFu, theta, L);
+          int kept = compact_row<PER>(cand + rb, m, min(rank, m), nL, eL, cur, e4max, nullptr, thL, th, nullptr,
                                       FILTER_SLACK);
-          if (kept > C - TC_BN) kept = recompact_exact<PER>(cand + rb, kept, rank, nL, eL, ge, th);
+          if (kept > C - TC_BN) kept = recompact_exact<PER>(cand + rb, kept, rank, nL, eL, ge, th, th);
           if (lane == L) {
             theta = th;
             cnt = kept;
@@ -907,7 +874,8 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     const float n_i = nrm[r], e4_i = ge[r].y;
     RowRegs<PER> regs;
     load_row<PER>(cand + rb, m0, regs);
-    const int m = compact_row<PER>(cand + rb, m0, min(rank, m0), n_i, e4_i, regs, 0.0f, ge, th, &ukey);
+    const int m = compact_row<PER>(cand + rb, m0, min(rank, m0), n_i, e4_i, regs, 0.0f, ge, 3.402823466e+38f, th,
+                                   &ukey);
     band += static_cast<unsigned long long>(m);
     if (lane == 0) {
       cand_cnt[r] = m;

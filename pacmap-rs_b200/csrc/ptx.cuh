@@ -12,6 +12,12 @@ __device__ __forceinline__ uint64_t globaltimer() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+// *p = (a, b) when x >= y, as one predicated store (no branch, nothing written otherwise).
+__device__ __forceinline__ void st_global_v2_if_ge(void* p, uint32_t a, uint32_t b, float x, float y) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ge.f32 q, %3, %4;\n\t@q st.global.v2.u32 [%0], {%1, %2};\n\t}\n" ::"l"(p),
+               "r"(a), "r"(b), "f"(x), "f"(y)
+               : "memory");
+}
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
