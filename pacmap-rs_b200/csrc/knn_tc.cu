@@ -725,30 +725,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
     uint32_t n_ins = 0, n_comp = 0;  // this row's insertions and compactions (statistics)
     const int cnt0 = cnt;            // entries carried over from an earlier pass
     auto screen = [&](const uint32_t (&r)[32], int colb) {
+      const float* Dv = reinterpret_cast<const float*>(r);
       float m8[4];
 #pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        const float* D = reinterpret_cast<const float*>(r) + 8 * g;
-        m8[g] = fmax3(fmax3(D[0], D[1], D[2]), fmax3(D[3], D[4], D[5]), fmaxf(D[6], D[7]));
-      }
+      for (int g = 0; g < 4; ++g)
+        m8[g] = fmax3(fmax3(Dv[8 * g], Dv[8 * g + 1], Dv[8 * g + 2]), fmax3(Dv[8 * g + 3], Dv[8 * g + 4], Dv[8 * g + 5]),
+                      fmaxf(Dv[8 * g + 6], Dv[8 * g + 7]));
       const float m = fmaxf(fmax3(m8[0], m8[1], m8[2]), m8[3]);
       // v = -2 D <= theta exactly when D >= -theta / 2 (both scalings by 2 are exact)
       const float hth = -0.5f * theta;
       if (__any_sync(0xFFFFFFFFu, m >= hth)) {
+        // every column of the 32 without a branch: a predicated store of (j, v = -2 D) that also returns the
+        // count (a divergent branch per column, or a vote per 8 columns, cost more than the column's work)
 #pragma unroll
-        for (int g = 0; g < 4; ++g) {
-          if (__any_sync(0xFFFFFFFFu, m8[g] >= hth)) {
-            // every column of the group without a branch: a predicated store of (j, v = -2 D) and a
-            // predicated count (a divergent branch per column cost more than the column's work)
-#pragma unroll
-            for (int c = 8 * g; c < 8 * g + 8; ++c) {
-              const float D = __uint_as_float(r[c]);
-              st_global_v2_if_ge(cand + cbase + cnt, static_cast<uint32_t>(colb + c), __float_as_uint(-2.0f * D), D,
-                                 hth);
-              cnt += D >= hth ? 1 : 0;
-            }
-          }
-        }
+        for (int c = 0; c < 32; ++c)
+          cnt += st_global_v2_if_ge(cand + cbase + cnt, static_cast<uint32_t>(colb + c), __float_as_uint(-2.0f * Dv[c]),
+                                    Dv[c], hth);
       }
     };
     for (int t = 0; t < nt; ++t) {

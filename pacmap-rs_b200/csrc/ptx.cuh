@@ -12,11 +12,16 @@ __device__ __forceinline__ uint64_t globaltimer() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// *p = (a, b) when x >= y, as one predicated store (no branch, nothing written otherwise).
-__device__ __forceinline__ void st_global_v2_if_ge(void* p, uint32_t a, uint32_t b, float x, float y) {
-  asm volatile("{\n\t.reg .pred q;\n\tsetp.ge.f32 q, %3, %4;\n\t@q st.global.v2.u32 [%0], {%1, %2};\n\t}\n" ::"l"(p),
-               "r"(a), "r"(b), "f"(x), "f"(y)
-               : "memory");
+// *p = (a, b) when x >= y, as one predicated store (no branch, nothing written otherwise); returns 1 when
+// it stored, else 0 (the same predicate, not a second comparison).
+__device__ __forceinline__ uint32_t st_global_v2_if_ge(void* p, uint32_t a, uint32_t b, float x, float y) {
+  uint32_t stored;
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ge.f32 q, %4, %5;\n\t@q st.global.v2.u32 [%1], {%2, %3};\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(stored)
+      : "l"(p), "r"(a), "r"(b), "f"(x), "f"(y)
+      : "memory");
+  return stored;
 }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
