@@ -386,7 +386,34 @@ __global__ void absmax_kernel(const float* __restrict__ x, uint64_t total, uint3
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
-// Also writes xperm (n x d, rows in the locality order), which the exact re-rank gathers from.
+// The re-rank copy of x: rows in the locality order, each in the lane-grouped layout of the reference's
+// eight-lane distance sum (distance.rs:50-75, lane l adds elements l, l + 8, l + 16, ... in turn): lane l's
+// terms 4k .. 4k+3 (elements 8 (4k + q) + l) sit at floats 32 k + 4 l + q, zeros past the last full chunk
+// of 8, then the d % 8 remainder in order, the row padded to a multiple of 4 floats. An 8-lane group
+// reads one 128-byte run per 16-byte load, and each lane still adds its own terms in the reference's
+// order (an added zero term leaves an f32 sum unchanged).
+struct RerankLayout {
+  int nc, nq, tail, ds;  // chunks of 8, groups of 4 chunks, remainder, row stride (floats)
+};
+__host__ __device__ __forceinline__ RerankLayout rerank_layout(int d) {
+  RerankLayout L;
+  L.nc = d / 8;
+  L.nq = (L.nc + 3) / 4;
+  L.tail = d % 8;
+  L.ds = 32 * L.nq + ((L.tail + 3) & ~3);
+  return L;
+}
+// The element of x stored at float o of a row in this layout, -1 for padding.
+__device__ __forceinline__ int rerank_src(const RerankLayout& L, int o) {
+  if (o < 32 * L.nq) {
+    const int k = o >> 5, l = (o & 31) >> 2, q = o & 3, p = 4 * k + q;
+    return p < L.nc ? 8 * p + l : -1;
+  }
+  const int t = o - 32 * L.nq;
+  return t < L.tail ? 8 * L.nc + t : -1;
+}
+
+// Also writes xperm (n rows in the locality order, RerankLayout), which the exact re-rank gathers from.
 template <bool BF16>
 __global__ void split_rows_kernel(const float* __restrict__ x, const uint32_t* __restrict__ perm, uint64_t n, int d,
                                   int KP, uint64_t n_pad, float s, uint16_t* __restrict__ H, float* __restrict__ nrm,
@@ -402,7 +429,6 @@ __global__ void split_rows_kernel(const float* __restrict__ x, const uint32_t* _
       float xs = 0.0f;
       if (r < n && c < d) {
         const float xv = x[src * d + c];
-        xperm[r * d + c] = xv;
         xs = xv * s;
       }
       uint16_t hbits;
@@ -421,6 +447,13 @@ __global__ void split_rows_kernel(const float* __restrict__ x, const uint32_t* _
       nn = fmaf(xs, xs, nn);
       aa = fmaf(hf, hf, aa);
       bb = fmaf(l, l, bb);
+    }
+    if (r < n) {
+      const RerankLayout L = rerank_layout(d);
+      for (int o = lane; o < L.ds; o += 32) {
+        const int c = rerank_src(L, o);
+        xperm[r * L.ds + o] = c >= 0 ? x[src * d + c] : 0.0f;
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -884,11 +917,22 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
 }
 
 // 3b. exact re-rank of the compacted band: the reference's f32 distance of every survivor (8-lane
-//     groups in distance.rs:50-75's lane order, 4 survivors per warp pass, row i of x in registers
-//     when it has at most 8 * NC elements, else read from L1 each pass with NC = 0), sorted by
-//     (distance, index); output at the original row, original indices.
-// x: the rows in the locality order (row r is point perm[r]); candidates of nearby rows sit nearby.
-template <int PER, int WARPS, int NC>
+//     groups in distance.rs:50-75's lane order, each lane reading its terms four at a time from the
+//     lane-grouped rows, 4 survivors per warp pass, row i of x in registers when it has at most 4 NQ
+//     chunks of 8, else read from L1 each pass with NQ = 0), sorted by (distance, index); output at the
+//     original row, original indices.
+// x: the rows in the locality order (row r is point perm[r]) in RerankLayout; candidates of nearby rows
+// sit nearby.
+__device__ __forceinline__ float add_sq4(float acc, const float4 a, const float4 b) {
+  const float d0 = __fsub_rn(a.x, b.x), d1 = __fsub_rn(a.y, b.y), d2 = __fsub_rn(a.z, b.z), d3 = __fsub_rn(a.w, b.w);
+  acc = __fadd_rn(acc, __fmul_rn(d0, d0));
+  acc = __fadd_rn(acc, __fmul_rn(d1, d1));
+  acc = __fadd_rn(acc, __fmul_rn(d2, d2));
+  return __fadd_rn(acc, __fmul_rn(d3, d3));
+}
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+template <int PER, int WARPS, int NQ>
 __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
     const float* __restrict__ x, uint64_t n, int d, int K, const uint32_t* __restrict__ perm,
     const uint2* __restrict__ cand, const int* __restrict__ cand_cnt, uint32_t* __restrict__ out_idx,
@@ -898,17 +942,18 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint64_t* keys = keys_all[warp];
   const int l8 = lane & 7, grp = lane >> 3;
-  const int nc = d >> 3;
+  const RerankLayout lay = rerank_layout(d);
+  const int nq = lay.nq, tail0 = 32 * lay.nq;
   for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * WARPS + warp; r < n;
        r += static_cast<uint64_t>(gridDim.x) * WARPS) {
     const int m = min(cand_cnt[r], C);
     if (m < 0) continue;  // overflowed in the filter: handled by the exact fallback
     const uint64_t rb = r * static_cast<uint64_t>(C);
     const uint64_t orow = perm[r];
-    const float* a = x + r * d;
-    float ra[NC > 0 ? NC : 1];
+    const float* a = x + r * lay.ds;
+    float4 ra[NQ > 0 ? NQ : 1];
 #pragma unroll
-    for (int ch = 0; ch < NC; ++ch) ra[ch] = ch < nc ? a[8 * ch + l8] : 0.0f;
+    for (int k = 0; k < NQ; ++k) ra[k] = k < nq ? ld4(a + 32 * k + 4 * l8) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     int nk = 0;
     // 32 candidates per chunk: their indices and original ids by one coalesced and one parallel load, then
     // two candidates per 8-lane group and pass, both rows' loads issued before either sum
@@ -928,30 +973,30 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
           j2[h] = __shfl_sync(0xFFFFFFFFu, my_j, q & 31);
           real2[h] = (q < span) && (jp2[h] != r);
         }
-        const float* b0 = x + static_cast<uint64_t>(jp2[0]) * d;
-        const float* b1 = x + static_cast<uint64_t>(jp2[1]) * d;
+        const float* b0 = x + static_cast<uint64_t>(jp2[0]) * lay.ds;
+        const float* b1 = x + static_cast<uint64_t>(jp2[1]) * lay.ds;
         float acc0 = 0.0f, acc1 = 0.0f;
-        if (NC > 0) {
-          float v0[NC > 0 ? NC : 1], v1[NC > 0 ? NC : 1];
+        if (NQ > 0) {
+          float4 v0[NQ > 0 ? NQ : 1], v1[NQ > 0 ? NQ : 1];
 #pragma unroll
-          for (int ch = 0; ch < NC; ++ch) {
-            v0[ch] = ch < nc ? b0[8 * ch + l8] : 0.0f;
-            v1[ch] = ch < nc ? b1[8 * ch + l8] : 0.0f;
+          for (int k = 0; k < NQ; ++k) {
+            if (k < nq) {
+              v0[k] = ld4(b0 + 32 * k + 4 * l8);
+              v1[k] = ld4(b1 + 32 * k + 4 * l8);
+            }
           }
 #pragma unroll
-          for (int ch = 0; ch < NC; ++ch) {
-            if (ch < nc) {
-              const float d0 = __fsub_rn(ra[ch], v0[ch]), d1 = __fsub_rn(ra[ch], v1[ch]);
-              acc0 = __fadd_rn(acc0, __fmul_rn(d0, d0));
-              acc1 = __fadd_rn(acc1, __fmul_rn(d1, d1));
+          for (int k = 0; k < NQ; ++k) {
+            if (k < nq) {
+              acc0 = add_sq4(acc0, ra[k], v0[k]);
+              acc1 = add_sq4(acc1, ra[k], v1[k]);
             }
           }
         } else {
-          for (int ch = 0; ch < nc; ++ch) {
-            const float av = a[8 * ch + l8];
-            const float d0 = __fsub_rn(av, b0[8 * ch + l8]), d1 = __fsub_rn(av, b1[8 * ch + l8]);
-            acc0 = __fadd_rn(acc0, __fmul_rn(d0, d0));
-            acc1 = __fadd_rn(acc1, __fmul_rn(d1, d1));
+          for (int k = 0; k < nq; ++k) {
+            const float4 av = ld4(a + 32 * k + 4 * l8);
+            acc0 = add_sq4(acc0, av, ld4(b0 + 32 * k + 4 * l8));
+            acc1 = add_sq4(acc1, av, ld4(b1 + 32 * k + 4 * l8));
           }
         }
         t2[0] = 0.0f;
@@ -961,9 +1006,9 @@ __global__ void __launch_bounds__(WARPS * 32) knn_rerank_kernel(
           t2[0] = __fadd_rn(t2[0], __shfl_sync(0xFFFFFFFFu, acc0, (lane & ~7) + l));
           t2[1] = __fadd_rn(t2[1], __shfl_sync(0xFFFFFFFFu, acc1, (lane & ~7) + l));
         }
-        for (int q = nc * 8; q < d; ++q) {
-          const float av = a[q];
-          const float d0 = __fsub_rn(av, b0[q]), d1 = __fsub_rn(av, b1[q]);
+        for (int q = 0; q < lay.tail; ++q) {
+          const float av = a[tail0 + q];
+          const float d0 = __fsub_rn(av, b0[tail0 + q]), d1 = __fsub_rn(av, b1[tail0 + q]);
           t2[0] = __fadd_rn(t2[0], __fmul_rn(d0, d0));
           t2[1] = __fadd_rn(t2[1], __fmul_rn(d1, d1));
         }
@@ -1157,7 +1202,7 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
   if (nprobe > 0 && nprobe < PIV) probe_lists(nprobe, 0xFFFFFFFFu, tile_ptr, tile_list);
 
   DevBuf<uint16_t> H(c, n_pad * KP);
-  DevBuf<float> xperm(c, n * d);
+  DevBuf<float> xperm(c, n * static_cast<uint64_t>(rerank_layout(static_cast<int>(d)).ds));
   DevBuf<float> nrm(c, n_pad), A(c, n_pad), B(c, n_pad);
   DevBuf<float2> ge(c, n_pad);
   DevBuf<uint16_t> gq(c, n_pad * 16);
@@ -1327,16 +1372,17 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     kern<<<rgrid, warps * 32, 0, c.stream>>>(xperm.get(), n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
                                              d_dist, fbk.get(), fbk.get() + n);
   };
+  // NQ groups of four chunks of 8 in registers: d < 8 * 4 NQ + 8 (the remainder is read separately)
   if (PER == 16) {
     if (d > 256) rerank(knn_rerank_kernel<16, 8, 0>, 8);
-    else if (d > 128) rerank(knn_rerank_kernel<16, 8, 32>, 8);
-    else if (d > 64) rerank(knn_rerank_kernel<16, 8, 16>, 8);
-    else rerank(knn_rerank_kernel<16, 8, 8>, 8);
+    else if (d > 128) rerank(knn_rerank_kernel<16, 8, 8>, 8);
+    else if (d > 64) rerank(knn_rerank_kernel<16, 8, 4>, 8);
+    else rerank(knn_rerank_kernel<16, 8, 2>, 8);
   } else {
     if (d > 256) rerank(knn_rerank_kernel<32, 4, 0>, 4);
-    else if (d > 128) rerank(knn_rerank_kernel<32, 4, 32>, 4);
-    else if (d > 64) rerank(knn_rerank_kernel<32, 4, 16>, 4);
-    else rerank(knn_rerank_kernel<32, 4, 8>, 4);
+    else if (d > 128) rerank(knn_rerank_kernel<32, 4, 8>, 4);
+    else if (d > 64) rerank(knn_rerank_kernel<32, 4, 4>, 4);
+    else rerank(knn_rerank_kernel<32, 4, 2>, 4);
   }
   PM_LAUNCHED();
 
