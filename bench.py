@@ -55,9 +55,9 @@ MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant kernels at the
 # 1,000,000 x 128 workload, from one-pass captures (ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
 # -k regex:<kernel> -s <launches to skip> on `bench.py --minimal --steps 1 --warmup 1`): the filter's main
-# pass (the launch its roofline times; the bound pass moves 15.4 GB, mostly candidate writes), and the
+# pass (the launch its roofline times; the bound pass moves 16.9 GB, mostly candidate writes), and the
 # gradient's average over the (0, 50, 150) schedule (1.182 GB per phase-2 launch, 1.143 GB per phase-3).
-TRAFFIC = {"knn_filter_kernel": 5374556672, "grad_adam_kernel": 1152481088}
+TRAFFIC = {"knn_filter_kernel": 5133694464, "grad_adam_kernel": 1152481088}
 
 
 def _peaks():
@@ -460,8 +460,8 @@ def run_ours(args, rank, world, local_rank):
                 "exact_knn_stage_ms": round(sl.get("knn", 0.0), 3),
                 "full_square_equivalent_tflops": round(2.0 * n * n * d / (sl["knn"] * 1e-3) / 1e12, 1) if sl.get("knn") else None,
                 "bound_by": ("the epilogue's candidate screening and insertion (per row: %.0f insertions, %.1f "
-                             "compactions, %.0f candidates left for the exact re-rank); the tensor pipe is busy a few "
-                             "per cent of the launch" % (sl.get("knn_insertions_per_row", 0.0),
+                             "compactions, %.0f candidates left for the exact re-rank); the tensor pipe is busy about "
+                             "15 per cent of the main pass (ncu, 300,000 rows)" % (sl.get("knn_insertions_per_row", 0.0),
                                                          sl.get("knn_compactions_per_row", 0.0),
                                                          sl.get("knn_band_per_row", 0.0)))}
     opt_ms = sl.get("optimize", 0.0)
