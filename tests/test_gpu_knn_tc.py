@@ -20,6 +20,8 @@ def _mix(n, d, seed):
 @pytest.mark.parametrize("mode", [F16, BF16])
 @pytest.mark.parametrize("n,d,k", [(3001, 128, 90), (2000, 100, 60), (4096, 32, 17), (777, 13, 90), (300, 64, 10),
                                    (1024, 128, 1), (513, 65, 200),
+                                   # fewer columns than one chunk of the reference's eight distance lanes
+                                   (900, 5, 20),
                                    # resident A, one K block per stage (d 129..256)
                                    (700, 130, 17), (4100, 192, 99), (2000, 256, 90),
                                    # A and B streamed per K block (d > 256), ragged last block included
