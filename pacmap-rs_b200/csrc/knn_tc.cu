@@ -136,7 +136,7 @@ __device__ __forceinline__ void load_row(const uint2* __restrict__ cand, int m, 
 // threshold of the same row (every theta is at or above the row's final one, so the band keeps every
 // neighbour; the entries that defined the smaller of the two all pass it, so at least `rank` are kept).
 // slack > 0 ends the bisection at the first key T with rank <= #{keys <= T} <= rank + slack: T is then at or
-// above the rank-th smallest key (a looser bound for fewer serial steps; the final compaction is exact).
+// above the rank-th smallest key (a looser bound, and a band a few entries larger, for fewer serial steps).
 template <int PER>
 __device__ __forceinline__ int compact_row(uint2* __restrict__ cand, int m, int rank, float n_i, float e4_i,
                                            const RowRegs<PER>& r, float e4max, const float2* __restrict__ ge,
@@ -871,9 +871,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_filter_kernel(
 // ---------------------------------------------------------------------------------------------
 // 3a. final compaction: the row's certified band (v <= theta of its rank-th upper bound), one warp
 //     per row; the count is written back (rows that overflowed in the filter keep -1).
-//     With ub (the tile pruning's first pass): ub[r] = the rank-th smallest upper bound of the reference's
-//     squared distance (scaled by s^2) over the columns the row met, u + n_i + 2 e_i rounded up -- an
-//     upper bound of its k'-th neighbour distance, since k' of those rank columns are other points;
+//     With ub (the tile pruning's first pass): ub[r] = an upper bound at or above the rank-th smallest upper
+//     bound of the reference's squared distance (scaled by s^2) over the columns the row met, u + n_i + 2 e_i
+//     rounded up -- an upper bound of its k'-th neighbour distance, since k' of those rank columns are
+//     other points;
 //     +inf when the row met fewer than rank columns or overflowed.
 constexpr int RC_WARPS = 4;
 
@@ -899,8 +900,10 @@ __global__ void __launch_bounds__(RC_WARPS * 32) knn_compact_kernel(
     const float n_i = nrm[r], e4_i = ge[r].y;
     RowRegs<PER> regs;
     load_row<PER>(cand + rb, m0, regs);
+    // the early exit leaves ukey at or above the rank-th smallest upper bound: ub and theta stay valid
+    // bounds and the band a superset of the exact one (the re-rank's result is the same)
     const int m = compact_row<PER>(cand + rb, m0, min(rank, m0), n_i, e4_i, regs, 0.0f, ge, 3.402823466e+38f, th,
-                                   &ukey);
+                                   &ukey, FILTER_SLACK);
     band += static_cast<unsigned long long>(m);
     if (lane == 0) {
       cand_cnt[r] = m;
