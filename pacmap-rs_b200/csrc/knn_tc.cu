@@ -216,12 +216,24 @@ __device__ __noinline__ int recompact_exact(uint2* __restrict__ cand, int m, int
 // stores |p|^2 - 2 x.p of every (point, pivot) pair, and block 0 stores |p|^2 in `pnorm` (the tile
 // pruning's pivot distances).
 constexpr int PA_PTS = 64, PA_PIV = 128, PA_D = 32;
+constexpr int PA_XS = PA_PTS + 1;  // odd row stride: the transposed writes of x fall in 32 different banks
+
+// The pivots transposed, pT[c * PIV + p] = x[piv_rows[p]][c], zero for d <= c < dpad (dpad = d rounded up to
+// PA_D): every block of the assignment then stages its pivot slices with plain 16-byte copies.
+__global__ void pivots_t_kernel(const float* __restrict__ x, const uint32_t* __restrict__ piv_rows, int d, int dpad,
+                                float* __restrict__ pT) {
+  const uint64_t e = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= static_cast<uint64_t>(dpad) * PIV) return;
+  const int c = static_cast<int>(e / PIV), p = static_cast<int>(e % PIV);
+  pT[e] = c < d ? x[static_cast<uint64_t>(piv_rows[p]) * d + c] : 0.0f;
+}
+
 __global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restrict__ x, uint64_t n, int d,
-                                                           const uint32_t* __restrict__ piv_rows,
+                                                           const float* __restrict__ pT,
                                                            uint32_t* __restrict__ cell, float* __restrict__ score,
                                                            float* __restrict__ pnorm) {
-  __shared__ float xs[PA_D][PA_PTS + 4];  // [dim][point]
-  __shared__ float ps[PA_D][PA_PIV + 4];  // [dim][pivot]
+  __shared__ float xs[PA_D * PA_XS];                // [dim][point]
+  __shared__ __align__(16) float ps[PA_D][PA_PIV];  // [dim][pivot]
   __shared__ float pn[PA_PIV];
   __shared__ float best_s[PA_PTS][16];
   __shared__ uint32_t best_i[PA_PTS][16];
@@ -242,12 +254,12 @@ __global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restri
       for (int e = threadIdx.x; e < PA_D * PA_PTS; e += 256) {
         const int pi = e / PA_D, cc = e % PA_D;
         const uint64_t r = pt0 + pi;
-        xs[cc][pi] = (r < n && c0 + cc < d) ? x[r * d + c0 + cc] : 0.0f;
+        xs[cc * PA_XS + pi] = (r < n && c0 + cc < d) ? x[r * d + c0 + cc] : 0.0f;
       }
-      for (int e = threadIdx.x; e < PA_D * PA_PIV; e += 256) {
-        const int pv = e / PA_D, cc = e % PA_D;
-        const uint64_t prow = piv_rows[half * PA_PIV + pv];
-        ps[cc][pv] = (c0 + cc < d) ? x[prow * d + c0 + cc] : 0.0f;
+      for (int e = threadIdx.x; e < PA_D * PA_PIV / 4; e += 256) {
+        const int cc = e / (PA_PIV / 4), v = e % (PA_PIV / 4);
+        reinterpret_cast<float4*>(&ps[cc][0])[v] =
+            __ldg(reinterpret_cast<const float4*>(pT + static_cast<uint64_t>(c0 + cc) * PIV + half * PA_PIV) + v);
       }
       __syncthreads();
       if (threadIdx.x < PA_PIV)
@@ -256,7 +268,7 @@ __global__ void __launch_bounds__(256) pivot_assign_kernel(const float* __restri
       for (int cc = 0; cc < PA_D; ++cc) {
         float xv[4], pv[8];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) xv[i] = xs[cc][tp * 4 + i];
+        for (int i = 0; i < 4; ++i) xv[i] = xs[cc * PA_XS + tp * 4 + i];
 #pragma unroll
         for (int j = 0; j < 8; ++j) pv[j] = ps[cc][tq * 8 + j];
 #pragma unroll
@@ -1130,7 +1142,13 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
     score.alloc(c, n * PIV);
     pnorm.alloc(c, PIV);
   }
-  pivot_assign_kernel<<<ceil_div(n, PA_PTS), 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), piv_rows.get(), cell.get(),
+  const int dpad = static_cast<int>((d + PA_D - 1) / PA_D * PA_D);
+  DevBuf<float> pT(c, static_cast<uint64_t>(dpad) * PIV);
+  pivots_t_kernel<<<ceil_div(static_cast<uint64_t>(dpad) * PIV, 256), 256, 0, c.stream>>>(d_x, piv_rows.get(),
+                                                                                          static_cast<int>(d), dpad,
+                                                                                          pT.get());
+  PM_LAUNCHED();
+  pivot_assign_kernel<<<ceil_div(n, PA_PTS), 256, 0, c.stream>>>(d_x, n, static_cast<int>(d), pT.get(), cell.get(),
                                                                  score.get(), pnorm.get());
   PM_LAUNCHED();
   cell_chunk_count_kernel<<<chunks, 256, 0, c.stream>>>(cell.get(), n, cell_counts.get());
