@@ -21,7 +21,8 @@
 //     Any true neighbour has LB <= k'-th UB, so it is never dropped. From 32,768 rows the tile pruning
 //     (knn_prune.cu) restricts each row block to the column tiles that may hold one of its neighbours.
 //  3. knn_rerank_kernel: the final threshold, then the reference's exact f32 distance of every
-//     survivor, sorted by (distance, index): the rows of knn.rs.
+//     survivor (gathered from a lane-grouped copy of x by 16-byte loads, each lane adding its terms in
+//     the reference's order), sorted by (distance, index): the rows of knn.rs.
 //  Rows whose candidate band does not fit the buffer (e.g. thousands of exact duplicates) are
 //  recomputed by the exact SIMT kernel.
 //
