@@ -119,10 +119,28 @@ __global__ void __launch_bounds__(256) csr_fwd_fill_kernel(const uint32_t* __res
   }
 }
 
+// Reverse entries: pair (a, b) puts a into b's segment at a cursor taken by atomicAdd. Four pairs per round
+// have their atomics in flight together (a thread would otherwise wait one round trip per pair); the
+// order inside a segment is the atomics' and is sorted afterwards.
 __global__ void csr_rev_fill_kernel(const uint32_t* __restrict__ pairs, uint64_t P, int type, uint64_t n,
                                     uint32_t* __restrict__ cursor, uint32_t* __restrict__ col) {
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += stride) {
+  uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; p + 3 * stride < P; p += 4 * stride) {
+    uint32_t a[4], b[4], pos[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      a[k] = pairs[2 * (p + k * stride)];
+      b[k] = pairs[2 * (p + k * stride) + 1];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      pos[k] = (b[k] < n && a[k] != b[k]) ? atomicAdd(&cursor[static_cast<uint64_t>(b[k]) * 3 + type], 1u) : 0u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (b[k] < n && a[k] != b[k]) col[pos[k]] = a[k];
+  }
+  for (; p < P; p += stride) {
     const uint32_t a = pairs[2 * p], b = pairs[2 * p + 1];
     if (b < n && a != b) col[atomicAdd(&cursor[static_cast<uint64_t>(b) * 3 + type], 1u)] = a;
   }
