@@ -18,7 +18,8 @@ struct Ctx {
 };
 
 // Stream-ordered device allocation (cudaMallocAsync on the call's stream; the device pool keeps freed
-// blocks cached, so repeated calls do not pay for allocation).
+// blocks cached, so repeated calls do not pay for allocation). Every buffer starts on a 256-byte boundary,
+// as cudaMalloc's do: the TMA tensor maps and the 16-byte vector loads rely on it.
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
