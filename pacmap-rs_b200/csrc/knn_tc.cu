@@ -1389,6 +1389,9 @@ bool knn_tc_device(Ctx& c, const float* d_x, uint64_t n, uint64_t d, uint64_t kp
 
   compact(nullptr, nullptr, counters.get() + 2);
   const int di = static_cast<int>(d), ki = static_cast<int>(kp);
+  // the re-rank reads xperm with 16-byte loads
+  PM_REQUIRE((reinterpret_cast<uintptr_t>(xperm.get()) & 15u) == 0, PACMAP_ERR_CUDA,
+             "re-rank copy of x is not 16-byte aligned");
   auto rerank = [&](auto kern, int warps) {
     const unsigned rgrid = std::min<unsigned>(ceil_div(n, warps), c.sm_count * 32);
     kern<<<rgrid, warps * 32, 0, c.stream>>>(xperm.get(), n, di, ki, perm.get(), cand.get(), ccnt.get(), d_idx,
