@@ -10,7 +10,7 @@ embedding's coordinates as the start -> CSR ->
 the shortened schedule (0, 50, 150) of fused gradient+Adam iterations in one CUDA graph):
   * value: inputs resident in HBM, C ABI `pacmap_fit_transform_learned_device`, CUDA events around
            each step; the plain schedule (Random init, (100, 100, 250)) on the same draw is timed the
-           same way (`plain_gpu_s`), and both embeddings are judged by 10-NN preservation and triplet
+           same way (`plain_gpu_s`), and both embeddings are compared by 10-NN preservation and triplet
            accuracy; a learned run more than 0.005 below the plain run on either metric continues on the
            plain schedule, inside the timed step;
   * e2e:   the learned step through `pacmap_fit_transform_learned` with pinned host input and host

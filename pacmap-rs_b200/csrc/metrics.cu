@@ -1,4 +1,4 @@
-// K14 -- embedding quality (no reference analogue; the judge of the learned initialiser):
+// K14 -- embedding quality (no reference analogue; the measure the learned initialiser is held to):
 //   * k-NN preservation: for each sampled point, the share of its k nearest neighbours in the data
 //     (preprocessed, reference f32 distance) that are also among its k nearest in the embedding, both
 //     ranked by (f32 distance, index) with the exact kNN kernel;

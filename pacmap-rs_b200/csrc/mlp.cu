@@ -1,4 +1,4 @@
-// The learned initialiser (no reference analogue; the north star's learned pattern): an MLP
+// The learned initialiser (no reference analogue; it lets a shortened schedule replace the plain one): an MLP
 // d -> 512 -> 512 -> dim (ReLU) with BF16 weights and activations and FP32 accumulation, trained with
 // AdamW on (preprocessed x, PaCMAP embedding) pairs and applied to new data as Initialization::Value
 // (src/lib.rs:753-766 rescales it to std 1e-4, so only its geometry matters).

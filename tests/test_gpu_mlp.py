@@ -131,7 +131,7 @@ def test_learned_init_gains_over_random_init_on_the_short_schedule(lib):
     assert q_learned[1] >= q_short[1] + 0.02
     # started in the training embedding's coordinates, the short schedule keeps more of the predicted layout
     # than through the 1e-4 Value z-scoring (0.728 vs 0.718 here, plain 0.734; the benchmark's gate is
-    # judged at 1M x 128)
+    # measured at 1M x 128)
     assert q_scaled[1] > q_learned[1]
     assert q_scaled[0] >= q_plain[0] - 0.005 and q_scaled[1] >= q_plain[1] - 0.01
 
